@@ -1,0 +1,642 @@
+#!/usr/bin/env python3
+"""Benchmark of the cuckoo filter batch path on B200.
+
+Metric: Gkeys/s of insert + lookup (+ delete) at 95 % load, with each kernel's
+fraction of the HBM sector roofline.  One step = clear the filter, insertMany
+the fill keys (to 0.95 load), containsMany a 50 %-positive batch, deleteMany a
+batch of stored keys.
+
+Default workload ("large"): 2^31 slots, 16-bit tags, 16-slot buckets (4 GiB
+table), BFS eviction, maxEvictions 500, uint64 keys; fill = floor(0.95 * 2^31)
+keys from splitmix64(seed 3); 2^28 lookups = 2^27 stored keys sampled without
+replacement + 2^27 splitmix64(seed 4) keys that are not stored; 2^26 deletes
+(the first 2^26 sampled stored keys).  Every input is larger than the 126 MB L2.
+
+Legs of one run:
+  value       device-resident inputs; CUDA events around each step on the
+              launching stream; async C-ABI calls (one kernel per op).
+  e2e         the synchronous C-ABI calls (insertMany/containsMany/deleteMany)
+              with inputs copied from pinned host memory and results copied
+              back inside the timed region.
+  cpu_baseline the oracle's multithreaded CPU port on a bounded sample.
+
+`--impl reference` times the reference's algorithm on the host cores (the CPU
+port, all threads) on a bounded sample of the same workload and, where the
+reference's own CUDA kernels were built (oracle/_ref), those kernels on the
+full workload on this GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import random
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Gkeys/s insert & lookup at 95% load, % of HBM sector roofline; p99 req latency"
+
+G = 0x9E3779B97F4A7C15
+M1 = 0xBF58476D1CE4E5B9
+M2 = 0x94D049BB133111EB
+U64 = 1 << 64
+
+WORKLOADS = {
+    "large": dict(
+        desc="large out-of-L2 filter: 2^31 slots, 16-bit tags, 16-slot buckets (4 GiB), BFS, maxEvictions 500, "
+             "uint64 keys; fill 0.95 (splitmix64 seed 3); 2^28 lookups 50% positive; 2^26 deletes",
+        capacity=1 << 31, bits=16, bs=16, policy="BFS", max_ev=500, fill=0.95,
+        n_pos=1 << 27, n_neg=1 << 27, n_del=1 << 26, seed_fill=3, seed_neg=4, seed_sample=5),
+    "small": dict(
+        desc="small filter (L2-resident): 2^20 slots, 16-bit tags, 16-slot buckets, BFS; 996147 keys "
+             "(splitmix64 seed 1); lookups of all of them + 996147 negatives (seed 2); delete half",
+        capacity=1 << 20, bits=16, bs=16, policy="BFS", max_ev=500, fill=0.95,
+        n_pos=996147, n_neg=996147, n_del=996147 // 2, seed_fill=1, seed_neg=2, seed_sample=0),
+}
+
+
+def s64(x: int) -> int:
+    x %= U64
+    return x - U64 if x >= (1 << 63) else x
+
+
+# ------------------------------------------------------------------ inputs
+
+
+def splitmix64_torch(seed: int, first: int, n: int, out, chunk: int = 1 << 27):
+    """splitmix64 outputs first..first+n-1 of `seed` into an int64 tensor (any device).
+
+    Output i is mix(seed + (i+1) * 0x9E3779B97F4A7C15) with the published
+    splitmix64 finaliser; int64 arithmetic wraps modulo 2^64.
+    """
+    import torch
+
+    def lsr(z, s):
+        return (z >> s) & ((1 << (64 - s)) - 1)
+
+    for off in range(0, n, chunk):
+        m = min(chunk, n - off)
+        i = torch.arange(first + off + 1, first + off + 1 + m, device=out.device, dtype=torch.int64)
+        z = i * s64(G) + s64(seed)
+        z = (z ^ lsr(z, 30)) * s64(M1)
+        z = (z ^ lsr(z, 27)) * s64(M2)
+        out[off:off + m] = z ^ lsr(z, 31)
+    return out
+
+
+def negative_collisions(seed_pos: int, n_pos: int, seed_neg: int, n_neg: int) -> list[int]:
+    """Indices j of splitmix64(seed_neg) outputs equal to some splitmix64(seed_pos)
+    output with index < n_pos.  splitmix64 is a bijection of its state, so
+    outputs are equal iff states are: j collides with i = j + c (mod 2^64),
+    c = (seed_neg - seed_pos) / gamma (mod 2^64)."""
+    c = ((seed_neg - seed_pos) * pow(G, -1, U64)) % U64
+    out: list[int] = []
+    # i = (j + c) mod 2^64 < n_pos  <=>  j in [(-c) mod 2^64, (-c) mod 2^64 + n_pos), modulo 2^64
+    lo = (-c) % U64
+    for j0 in (lo, lo - U64):
+        a, b = max(0, j0), min(n_neg, j0 + n_pos)
+        if a < b:
+            out.extend(range(a, b))
+    return out
+
+
+def collides(seed_pos: int, n_pos: int, seed_neg: int, j: int) -> bool:
+    c = ((seed_neg - seed_pos) * pow(G, -1, U64)) % U64
+    return (j + c) % U64 < n_pos
+
+
+def make_inputs(w: dict, device, rank: int = 0):
+    """Device tensors: fill keys, query keys (positives and negatives shuffled), delete keys."""
+    import torch
+
+    seed_fill = w["seed_fill"] + 1000 * rank
+    seed_neg = w["seed_neg"] + 1000 * rank
+    n_fill = int(w["fill"] * w["capacity"])
+    fill = torch.empty(n_fill, dtype=torch.int64, device=device)
+    splitmix64_torch(seed_fill, 0, n_fill, fill)
+    n_pos, n_neg = w["n_pos"], w["n_neg"]
+    if n_pos >= n_fill:
+        pos = fill[:n_pos]
+    else:
+        # sample without replacement: j -> (a*j + b) mod n_fill, gcd(a, n_fill) = 1
+        r = random.Random(w["seed_sample"] + rank)
+        while True:
+            a = r.randrange(1, n_fill)
+            if math.gcd(a, n_fill) == 1:
+                break
+        b = r.randrange(0, n_fill)
+        j = torch.arange(n_pos, device=device, dtype=torch.int64)
+        pos = fill[(j * a + b) % n_fill]
+    neg = torch.empty(n_neg, dtype=torch.int64, device=device)
+    splitmix64_torch(seed_neg, 0, n_neg, neg)
+    bad = negative_collisions(seed_fill, n_fill, seed_neg, n_neg)
+    extra = n_neg
+    for j in bad:  # replace colliding negatives by later outputs of the same stream
+        while collides(seed_fill, n_fill, seed_neg, extra):
+            extra += 1
+        cand = torch.empty(1, dtype=torch.int64, device=device)
+        splitmix64_torch(seed_neg, extra, 1, cand)
+        extra += 1
+        neg[j] = cand[0]
+    g = torch.Generator(device=device)
+    g.manual_seed(w["seed_sample"] + 17 + rank)
+    query = torch.cat([pos, neg])
+    query = query[torch.randperm(query.numel(), generator=g, device=device)]
+    dele = pos[: w["n_del"]].clone()
+    return fill, query, dele, len(bad)
+
+
+# ------------------------------------------------------------------ helpers
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+_REGISTERED = []
+
+
+def pinned_empty(n: int, dtype):
+    """Host tensor in page-locked memory.  Registers an ordinary allocation
+    (cudaHostRegister) instead of using torch's pinned allocator, which rounds
+    sizes up to a power of two."""
+    import torch
+
+    t = torch.empty(n, dtype=dtype)
+    nbytes = t.numel() * t.element_size()
+    if nbytes and torch._C._cudart.cudaHostRegister(t.data_ptr(), nbytes, 0) == 0:
+        _REGISTERED.append(t)
+        return t
+    return torch.empty(n, dtype=dtype, pin_memory=True)
+
+
+def release_pinned() -> None:
+    import torch
+
+    while _REGISTERED:
+        t = _REGISTERED.pop()
+        torch._C._cudart.cudaHostUnregister(t.data_ptr())
+
+
+def measured_peak() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------ CPU baselines
+
+
+def cpu_sample(scale_log2: int, threads: int, seed: int = 3) -> dict:
+    """The oracle's multithreaded port of the reference algorithm on the host:
+    a 2^scale_log2-slot filter (16/16, BFS) filled to 0.95, lookups of 2^(s-3)
+    keys (50 % positive), deletes of 2^(s-5) stored keys."""
+    import ctypes as C
+
+    import numpy as np
+
+    import oracle
+
+    cap = 1 << scale_log2
+    f = oracle.OracleFilter(key_bytes=8, bits=16, bucket_size=16, policy=oracle.POLICY_BFS, capacity=cap)
+    n_fill = int(0.95 * cap)
+    keys = oracle.splitmix64(seed, n_fill)
+    nq = 1 << (scale_log2 - 3)
+    q = np.concatenate([keys[: nq // 2], oracle.splitmix64(seed + 1, nq // 2)])
+    nd = 1 << (scale_log2 - 5)
+    out = np.empty(max(n_fill, nq), np.uint8)
+    L = oracle.lib()
+    t0 = time.perf_counter()
+    L.cfo_insert_mt(C.byref(f.p), f.table.ctypes.data, keys.ctypes.data, n_fill, None, threads)
+    t1 = time.perf_counter()
+    L.cfo_contains_mt(C.byref(f.p), f.table.ctypes.data, q.ctypes.data, nq, out.ctypes.data, threads)
+    t2 = time.perf_counter()
+    L.cfo_delete_mt(C.byref(f.p), f.table.ctypes.data, keys.ctypes.data, nd, None, threads)
+    t3 = time.perf_counter()
+    total = n_fill + nq + nd
+    return {"value": total / (t3 - t0) / 1e9, "unit": "Gkeys/s", "cores": threads, "kind": "port",
+            "sample": f"2^{scale_log2}-slot 16/16 BFS filter filled to 0.95 ({n_fill} keys), {nq} lookups "
+                      f"(50% positive), {nd} deletes; oracle/cf_oracle.c multithreaded port",
+            "insert_gkeys_s": n_fill / (t1 - t0) / 1e9, "contains_gkeys_s": nq / (t2 - t1) / 1e9,
+            "delete_gkeys_s": nd / (t3 - t2) / 1e9, "seconds": t3 - t0}
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------ GPU benchmark
+
+
+def run_b200(args, w: dict) -> dict | None:
+    import torch
+
+    from __graft_entry__ import package
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cfb = package()
+    stream = torch.cuda.current_stream()
+
+    cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=w["bits"], maxEvictions=w["max_ev"], blockSize=args.block,
+                           bucketSize=w["bs"], evictionPolicy=cfb.EvictionPolicy[w["policy"]])
+    f = cfb.CuckooFilter(cfg, w["capacity"])
+    fill, query, dele, n_coll = make_inputs(w, dev, rank)
+    n_fill, n_q, n_d = fill.numel(), query.numel(), dele.numel()
+    q_out = torch.empty(n_q, dtype=torch.bool, device=dev)
+    torch.cuda.synchronize()
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        f.clear(stream)  # synchronous memset of the table and counters
+        if ev:
+            ev[1].record(stream)
+        if args.sorted:
+            f.insertManySorted(fill, stream=stream)
+        else:
+            f.insertManyAsync(fill, stream=stream)
+        if ev:
+            ev[2].record(stream)
+        f.containsManyAsync(query, q_out, stream=stream)
+        if ev:
+            ev[3].record(stream)
+        f.deleteManyAsync(dele, stream=stream)
+        if ev:
+            ev[4].record(stream)
+
+    # warm-up; the first warm-up step also yields the exact sector accounting
+    acct = {}
+    for i in range(args.warmup):
+        f.clear(stream)
+        f.resetEvictionCount()
+        if args.sorted:
+            f.insertManySorted(fill, stream=stream)
+        else:
+            f.insertMany(fill, stream=stream)
+        st = f.stats()
+        if i == 0:
+            acct["i1_full"] = st["secondary"] + st["evicted_inserts"]
+            acct["inserted"] = st["occupied"]
+            acct["failed"] = st["failed"]
+            acct["evictions"] = st["evictions"]
+            acct["q_primary"] = f.probe_count(query, stream=stream)
+            acct["d_primary"] = f.probe_count(dele, stream=stream)
+        f.containsManyAsync(query, q_out, stream=stream)
+        f.deleteMany(dele, stream=stream)
+        if i == 0:
+            acct["removed"] = f.stats()["removed"]
+            acct["q_hits"] = int(q_out.sum().item())
+    torch.cuda.synchronize()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_wall0 = time.perf_counter()
+        for k in range(args.steps):
+            step(evs[k])
+        torch.cuda.synchronize()
+        t_wall1 = time.perf_counter()
+    barrier(world)
+    step_ms = [evs[k][0].elapsed_time(evs[k][4]) for k in range(args.steps)]
+    ins_ms = [evs[k][1].elapsed_time(evs[k][2]) for k in range(args.steps)]
+    con_ms = [evs[k][2].elapsed_time(evs[k][3]) for k in range(args.steps)]
+    del_ms = [evs[k][3].elapsed_time(evs[k][4]) for k in range(args.steps)]
+    total_ms = sum(step_ms)
+    total_ms_max = max_over_ranks(world, total_ms)
+    keys_per_step = n_fill + n_q + n_d
+    all_keys = sum_over_ranks(world, keys_per_step * args.steps)
+    value = all_keys / (total_ms_max / 1e3) / 1e9
+
+    peak, peak_src = measured_peak()
+    ins_bytes = n_fill * (8 + 32 + 32) + 32 * acct["i1_full"]
+    con_bytes = n_q * (8 + 1) + 32 * (2 * n_q - acct["q_primary"])
+    del_bytes = n_d * (8 + 1) + 32 * (2 * n_d - acct["d_primary"]) + 32 * acct["removed"]
+
+    def op(n, ms, b):
+        t = statistics.mean(ms) / 1e3
+        return {"gkeys_s": n / t / 1e9, "ms": statistics.mean(ms), "algorithmic_bytes": b,
+                "achieved_gbs": b / t / 1e9, "frac_of_hbm": b / t / 1e9 / peak}
+
+    ops = {"insert": op(n_fill, ins_ms, ins_bytes), "contains": op(n_q, con_ms, con_bytes),
+           "delete": op(n_d, del_ms, del_bytes), "clear_ms": statistics.mean(
+               [evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)])}
+    dom = max(("insert", "contains", "delete"), key=lambda k: ops[k]["ms"])
+    traffic = load_traffic(dom, w)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": ops[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": ops[dom]["achieved_gbs"] / peak, "peak_source": peak_src,
+            "traffic": traffic.get("bytes_per_launch") if traffic else None,
+            "traffic_source": traffic.get("source") if traffic else None}
+
+    # ------------------------------------------------ end to end (host buffers)
+    e2e = None
+    if not args.no_e2e:
+        h_fill = pinned_empty(n_fill, torch.int64)
+        h_query = pinned_empty(n_q, torch.int64)
+        h_del = pinned_empty(n_d, torch.int64)
+        h_out = pinned_empty(n_q, torch.bool)
+        h_fill.copy_(fill)
+        h_query.copy_(query)
+        h_del.copy_(dele)
+        d_fill = torch.empty_like(fill)
+        d_query = torch.empty_like(query)
+        d_del = torch.empty_like(dele)
+        torch.cuda.synchronize()
+        n_e2e = max(1, min(args.steps, args.e2e_steps))
+        times = []
+        for k in range(n_e2e + 1):
+            barrier(world)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            f.clear(stream)
+            d_fill.copy_(h_fill, non_blocking=True)
+            f.insertMany(d_fill, stream=stream)
+            d_query.copy_(h_query, non_blocking=True)
+            f.containsMany(d_query, q_out, stream=stream)
+            h_out.copy_(q_out, non_blocking=True)
+            d_del.copy_(h_del, non_blocking=True)
+            f.deleteMany(d_del, stream=stream)
+            torch.cuda.synchronize()
+            if k:  # first pass warms the pinned pages
+                times.append(time.perf_counter() - t0)
+        t = max_over_ranks(world, statistics.mean(times))
+        del h_fill, h_query, h_del, h_out
+        release_pinned()
+        e2e = {"value": all_keys / args.steps / t / 1e9, "unit": "Gkeys/s",
+               "h2d_bytes_per_step": 8 * keys_per_step, "d2h_bytes_per_step": n_q + 3 * 8 * 16,
+               "ms_per_step": t * 1e3, "steps": n_e2e,
+               "path": "synchronous C-ABI cf_insert/cf_contains/cf_delete, inputs copied from pinned host memory, "
+                       "lookup results copied back; wall clock per step"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(args.cpu_scale, host_threads())
+
+    st = f.stats()
+    result = None
+    if rank == 0:
+        result = {
+            "metric": METRIC, "value": value, "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: splitmix64 uint64 keys (seeded), positives sampled without replacement, "
+                    "negatives disjoint by construction",
+            "config": {"workload": args.workload, "desc": w["desc"], "capacity_slots": w["capacity"],
+                       "num_buckets": f.getNumBuckets(), "table_bytes": f.sizeInBytes(),
+                       "bits_per_tag": w["bits"], "bucket_size": w["bs"], "eviction": w["policy"],
+                       "max_evictions": w["max_ev"], "block_size": args.block,
+                       "insert_path": "insertManySorted" if args.sorted else "insertMany",
+                       "fill_keys": n_fill, "lookup_keys": n_q, "delete_keys": n_d,
+                       "negatives_replaced": n_coll,
+                       "l2": "inputs larger than L2 (table and key arrays exceed 126 MB); no flush needed"
+                       if w["capacity"] >= (1 << 26) else "table L2-resident (small workload)",
+                       "parallelism": f"{world} independent filter shard(s), one per GPU, no collective"},
+            "ops": ops,
+            "accounting": {**acct, "load_factor": acct["inserted"] / f.capacity()},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+            "wall_s_timed": t_wall1 - t_wall0,
+            "lost_tags": st["lost"],
+        }
+    f.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return result
+
+
+def load_traffic(kernel: str, w: dict) -> dict | None:
+    """Per-launch DRAM traffic of `kernel` from the committed ncu summary, scaled
+    from the captured case to this workload by keys processed."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+    except (OSError, ValueError):
+        return None
+    e = d.get(kernel)
+    if not e:
+        return None
+    n = {"insert": int(w["fill"] * w["capacity"]), "contains": w["n_pos"] + w["n_neg"], "delete": w["n_del"]}[kernel]
+    return {"bytes_per_launch": e["bytes_per_key"] * n, "source": e.get("source", p)}
+
+
+# ------------------------------------------------------------ reference arm
+
+
+def run_reference(args, w: dict) -> dict | None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    threads = host_threads()
+    steps = []
+    for _ in range(args.warmup):
+        cpu_sample(args.ref_scale, threads)
+    for _ in range(args.steps):
+        steps.append(cpu_sample(args.ref_scale, threads))
+    value = statistics.mean(s["value"] for s in steps)
+    sample = steps[0]
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gkeys/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(s["seconds"] for s in steps) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic: splitmix64 uint64 keys", "config": {"workload": args.workload, "desc": w["desc"]},
+        "cpu_baseline": {"value": value, "unit": "Gkeys/s", "cores": threads, "kind": "port",
+                         "sample": sample["sample"] + " (the reference's CPU cuckoo library is not vendored; "
+                                                      "this is the reference's GPU algorithm ported to host threads)"},
+        "e2e": {"value": value, "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "ops": {k: statistics.mean(s[k] for s in steps) for k in ("insert_gkeys_s", "contains_gkeys_s",
+                                                                  "delete_gkeys_s")},
+    }
+    if not args.no_ref_gpu:
+        out["reference_gpu"] = run_reference_gpu(args, w)
+    return out
+
+
+def run_reference_gpu(args, w: dict) -> dict:
+    """The reference's own CUDA kernels (compiled from its sources for sm_100a)
+    on the full workload, through its public API, timed with CUDA events."""
+    try:
+        import torch
+
+        import oracle
+    except ImportError as e:
+        return {"unavailable": str(e)}
+    if oracle.ref_gpu() is None or not torch.cuda.is_available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built or no GPU"}
+    pol = oracle.POLICY_BFS if w["policy"] == "BFS" else oracle.POLICY_DFS
+    try:
+        ref = oracle.RefGpuFilter(8, w["bits"], w["bs"], pol, w["max_ev"], w["capacity"])
+    except (KeyError, RuntimeError) as e:
+        return {"unavailable": f"configuration not instantiated: {e}"}
+    dev = torch.device("cuda", 0)
+    fill, query, dele, _ = make_inputs(w, dev)
+    out = torch.empty(query.numel(), dtype=torch.uint8, device=dev)
+    res = {"ins": [], "con": [], "del": []}
+    stream = torch.cuda.current_stream()
+    for k in range(args.warmup + args.steps):
+        ref.clear()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        ref.insert(fill.data_ptr(), fill.numel(), stream.cuda_stream or None, bool(args.sorted))
+        e[1].record(stream)
+        ref.contains(query.data_ptr(), query.numel(), out.data_ptr(), stream.cuda_stream or None)
+        e[2].record(stream)
+        ref.delete(dele.data_ptr(), dele.numel(), None, stream.cuda_stream or None)
+        e[3].record(stream)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            res["ins"].append(e[0].elapsed_time(e[1]))
+            res["con"].append(e[1].elapsed_time(e[2]))
+            res["del"].append(e[2].elapsed_time(e[3]))
+    occ = ref.occupied()
+    ref.close()
+    t = {k: statistics.mean(v) for k, v in res.items()}
+    n_total = fill.numel() + query.numel() + dele.numel()
+    return {"value": n_total / (sum(t.values()) / 1e3) / 1e9, "unit": "Gkeys/s",
+            "insert_gkeys_s": fill.numel() / t["ins"] * 1e3 / 1e9,
+            "contains_gkeys_s": query.numel() / t["con"] * 1e3 / 1e9,
+            "delete_gkeys_s": dele.numel() / t["del"] * 1e3 / 1e9,
+            "ms": t, "occupied_after": occ,
+            "build": "reference include/CuckooFilter.cuh compiled with -gencode arch=compute_100a,code=sm_100a "
+                     "(256-bit load path live), filter object in managed memory"}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large")
+    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--sorted", action="store_true", help="use insertManySorted for the fill")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--cpu-scale", type=int, default=27, help="log2 slots of the CPU-baseline sample")
+    ap.add_argument("--ref-scale", type=int, default=25, help="log2 slots of each reference-arm CPU step")
+    args = ap.parse_args()
+    if args.warmup < 1:
+        ap.error("--warmup must be >= 1")
+    w = WORKLOADS[args.workload]
+    res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

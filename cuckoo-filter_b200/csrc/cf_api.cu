@@ -1,0 +1,459 @@
+// cf_api.cu -- C ABI of the B200 cuckoo filter (declared in include/cuckoo_b200.h).
+//
+// Host side of the reference's CuckooFilter<Config> (CuckooFilter.cuh:140-785):
+// the filter owns its table and counters; the synchronous calls mirror the
+// reference's (launch, cudaStreamSynchronize, read the occupancy counter).  The
+// device-side filter descriptor is passed to kernels by value, never as a host
+// `this` pointer.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/cuckoo_b200.h"
+#include "cf_registry.cuh"
+
+using namespace cfb;
+
+struct cf_filter {
+    cf_config cfg;
+    const OpsTable* ops;
+    uint64_t num_buckets;
+    uint64_t table_bytes;
+    uint8_t* d_table;
+    unsigned long long* d_ctr;  // CTR_COUNT device counters
+    unsigned long long* h_ctr;  // pinned mirror
+    int device;
+    int block;
+    int max_grid[KID_COUNT_KERNELS];
+    int max_grid_aux;
+};
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int status, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? CF_ERR_NO_MEMORY : CF_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+}
+
+#define CF_CUDA(expr, what)                          \
+    do {                                             \
+        cudaError_t e_ = (expr);                     \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+const std::vector<OpsTable>& registry() {
+    static std::vector<OpsTable> v = [] {
+        std::vector<OpsTable> r;
+        register_bits8(r);
+        register_bits16(r);
+        register_bits32(r);
+        return r;
+    }();
+    return v;
+}
+
+const OpsTable* find_ops(const cf_config* c) {
+    for (const OpsTable& o : registry())
+        if (o.key_bytes == c->key_bytes && o.bits == c->bits_per_tag && o.bucket_size == c->bucket_size &&
+            o.word_bytes == c->word_bytes)
+            return &o;
+    return nullptr;
+}
+
+int validate(const cf_config* c) {
+    if (!c) return fail(CF_ERR_INVALID, "config is NULL");
+    if (c->key_bytes != 4 && c->key_bytes != 8) return fail(CF_ERR_INVALID, "key_bytes must be 4 or 8");
+    if (c->bits_per_tag != 8 && c->bits_per_tag != 16 && c->bits_per_tag != 32)
+        return fail(CF_ERR_INVALID, "bits_per_tag must be 8, 16 or 32");
+    if (c->bucket_size == 0 || (c->bucket_size & (c->bucket_size - 1)))
+        return fail(CF_ERR_INVALID, "bucket_size must be a power of two");
+    if (c->word_bytes != 8 && c->word_bytes != 4) return fail(CF_ERR_INVALID, "word_bytes must be 4 or 8");
+    if (c->eviction_policy != CF_EVICT_BFS && c->eviction_policy != CF_EVICT_DFS)
+        return fail(CF_ERR_INVALID, "eviction_policy must be CF_EVICT_BFS or CF_EVICT_DFS");
+    if (c->max_evictions < 1 || c->max_evictions > kMaxEvictionsCap)
+        return fail(CF_ERR_INVALID, "max_evictions must be in [1, %u]", kMaxEvictionsCap);
+    if (c->block_size != 0 && (c->block_size % 32 != 0 || c->block_size > 512))
+        return fail(CF_ERR_INVALID, "block_size must be 0 or a multiple of 32 up to 512");
+    if (c->alt_policy != CF_ALT_XOR) return fail(CF_ERR_UNSUPPORTED, "only the XOR alternate-bucket policy is built");
+    if (!find_ops(c))
+        return fail(CF_ERR_UNSUPPORTED, "no kernels for key_bytes=%u bits_per_tag=%u bucket_size=%u word_bytes=%u",
+                    c->key_bytes, c->bits_per_tag, c->bucket_size, c->word_bytes);
+    return CF_OK;
+}
+
+uint64_t num_buckets_for(uint64_t capacity, uint32_t bucket_size) {
+    // std::ceil((double)capacity / bucketSize), then nextPowerOfTwo (helpers.cuh:31-45).
+    const double req = std::ceil(static_cast<double>(capacity) / static_cast<double>(bucket_size));
+    uint64_t r = static_cast<uint64_t>(req);
+    if (r != 0 && (r & (r - 1)) == 0) return r;
+    uint64_t n = r - 1;
+    n |= n >> 1;
+    n |= n >> 2;
+    n |= n >> 4;
+    n |= n >> 8;
+    n |= n >> 16;
+    n |= n >> 32;
+    return n + 1;
+}
+
+DevTable dev(const cf_filter* f) { return DevTable{f->d_table, f->num_buckets - 1, f->d_ctr}; }
+
+LaunchCfg launch(const cf_filter* f, int kid, void* stream) {
+    return LaunchCfg{static_cast<cudaStream_t>(stream), f->block, f->max_grid[kid]};
+}
+
+LaunchCfg launch_aux(const cf_filter* f, void* stream) {
+    return LaunchCfg{static_cast<cudaStream_t>(stream), 256, f->max_grid_aux};
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int check_filter(const cf_filter* f) {
+    if (!f) return fail(CF_ERR_INVALID, "filter is NULL");
+    return CF_OK;
+}
+
+int check_batch(const cf_filter* f, const void* keys, uint64_t n) {
+    if (int s = check_filter(f)) return s;
+    if (n && !keys) return fail(CF_ERR_INVALID, "keys is NULL with n > 0");
+    return CF_OK;
+}
+
+// Synchronize, read the counters, surface device-side errors.
+int finish(cf_filter* f, void* stream, uint64_t* occupied_out) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CF_CUDA(cudaMemcpyAsync(f->h_ctr, f->d_ctr, CTR_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+            "counter read-back");
+    CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    if (f->h_ctr[CTR_ERROR] & ERR_CAS_LIMIT)
+        return fail(CF_ERR_DEVICE, "a compare-and-swap retry bound was hit on the device");
+    if (occupied_out) *occupied_out = f->h_ctr[CTR_OCCUPIED];
+    return CF_OK;
+}
+
+int do_insert(cf_filter* f, const void* keys, uint64_t n, uint8_t* out, void* stream) {
+    CF_CUDA(f->ops->insert(dev(f), keys, n, out, launch(f, KID_INSERT, stream),
+                           f->cfg.eviction_policy == CF_EVICT_BFS ? 1u : 0u, f->cfg.max_evictions),
+            "insert launch");
+    return CF_OK;
+}
+
+template <class C>
+void host_candidates_t(uint64_t mask, const void* keys, uint64_t n, uint64_t* i1, uint64_t* i2, uint32_t* fp) {
+    const auto* k = static_cast<const typename C::Key*>(keys);
+    for (uint64_t i = 0; i < n; ++i) {
+        uint64_t b;
+        uint32_t f;
+        candidates<C>(static_cast<uint64_t>(k[i]), mask, b, f);
+        if (i1) i1[i] = b;
+        if (i2) i2[i] = alt_bucket<C>(b, f, mask);
+        if (fp) fp[i] = f;
+    }
+}
+
+// Bucket size does not enter the hashing; 16 slots stands in for any.
+void host_candidates(uint32_t kb, uint32_t bits, uint64_t mask, const void* keys, uint64_t n, uint64_t* i1,
+                     uint64_t* i2, uint32_t* fp) {
+    if (kb == 8) {
+        if (bits == 8) host_candidates_t<Cfg<8, 8, 16, 8>>(mask, keys, n, i1, i2, fp);
+        else if (bits == 16) host_candidates_t<Cfg<8, 16, 16, 8>>(mask, keys, n, i1, i2, fp);
+        else host_candidates_t<Cfg<8, 32, 8, 8>>(mask, keys, n, i1, i2, fp);
+    } else {
+        if (bits == 8) host_candidates_t<Cfg<4, 8, 16, 8>>(mask, keys, n, i1, i2, fp);
+        else if (bits == 16) host_candidates_t<Cfg<4, 16, 16, 8>>(mask, keys, n, i1, i2, fp);
+        else host_candidates_t<Cfg<4, 32, 8, 8>>(mask, keys, n, i1, i2, fp);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cf_abi_version(void) { return CF_ABI_VERSION; }
+
+const char* cf_last_error(void) { return g_err; }
+
+const char* cf_status_string(int status) {
+    switch (status) {
+        case CF_OK: return "CF_OK";
+        case CF_ERR_INVALID: return "CF_ERR_INVALID";
+        case CF_ERR_UNSUPPORTED: return "CF_ERR_UNSUPPORTED";
+        case CF_ERR_CUDA: return "CF_ERR_CUDA";
+        case CF_ERR_NO_MEMORY: return "CF_ERR_NO_MEMORY";
+        case CF_ERR_DEVICE: return "CF_ERR_DEVICE";
+        case CF_ERR_NOT_LOADED: return "CF_ERR_NOT_LOADED";
+        default: return "CF_ERR_UNKNOWN";
+    }
+}
+
+int cf_config_supported(const cf_config* cfg) { return cfg && find_ops(cfg) != nullptr; }
+
+uint64_t cf_num_buckets_for(uint64_t capacity, uint32_t bucket_size) {
+    if (bucket_size == 0) return 0;
+    return num_buckets_for(capacity, bucket_size);
+}
+
+int cf_create(const cf_config* cfg, uint64_t capacity, cf_filter** out) {
+    if (!out) return fail(CF_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (int s = validate(cfg)) return s;
+    if (capacity == 0) return fail(CF_ERR_INVALID, "capacity must be > 0");
+    int device = 0;
+    {
+        cudaError_t e = cudaGetDevice(&device);
+        if (e != cudaSuccess) return fail(CF_ERR_NOT_LOADED, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    cf_filter* f = new cf_filter{};
+    f->cfg = *cfg;
+    f->ops = find_ops(cfg);
+    f->device = device;
+    f->num_buckets = num_buckets_for(capacity, cfg->bucket_size);
+    f->table_bytes = f->num_buckets * f->ops->bucket_bytes;
+    f->block = cfg->block_size ? static_cast<int>(cfg->block_size) : 256;
+    int sms = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    for (int k = 0; e == cudaSuccess && k < KID_COUNT_KERNELS; ++k) {
+        int bps = 0;
+        e = f->ops->occupancy(k, f->block, &bps);
+        f->max_grid[k] = sms * (bps > 0 ? bps : 1);
+    }
+    f->max_grid_aux = sms * 8;
+    if (e == cudaSuccess) e = cudaMalloc(&f->d_table, f->table_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&f->d_ctr, CTR_COUNT * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaHostAlloc(&f->h_ctr, CTR_COUNT * sizeof(unsigned long long), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMemset(f->d_table, 0, f->table_bytes);
+    if (e == cudaSuccess) e = cudaMemset(f->d_ctr, 0, CTR_COUNT * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        int s = cuda_fail(e, "filter allocation");
+        cf_destroy(f);
+        return s;
+    }
+    *out = f;
+    return CF_OK;
+}
+
+int cf_destroy(cf_filter* f) {
+    if (!f) return CF_OK;
+    DeviceGuard g(f->device);
+    if (f->d_table) cudaFree(f->d_table);
+    if (f->d_ctr) cudaFree(f->d_ctr);
+    if (f->h_ctr) cudaFreeHost(f->h_ctr);
+    delete f;
+    return CF_OK;
+}
+
+int cf_get_info(const cf_filter* f, cf_info* out) {
+    if (int s = check_filter(f)) return s;
+    if (!out) return fail(CF_ERR_INVALID, "out is NULL");
+    out->num_buckets = f->num_buckets;
+    out->capacity = f->num_buckets * f->cfg.bucket_size;
+    out->size_in_bytes = f->table_bytes;
+    out->bucket_bytes = f->ops->bucket_bytes;
+    out->device = f->device;
+    return CF_OK;
+}
+
+int cf_insert_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
+    if (int s = check_batch(f, d_keys, n)) return s;
+    DeviceGuard g(f->device);
+    return do_insert(f, d_keys, n, d_out, stream);
+}
+
+int cf_insert(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream, uint64_t* occupied_out) {
+    if (int s = check_batch(f, d_keys, n)) return s;
+    DeviceGuard g(f->device);
+    if (int s = do_insert(f, d_keys, n, d_out, stream)) return s;
+    return finish(f, stream, occupied_out);
+}
+
+int cf_insert_sorted(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,
+                     uint64_t* occupied_out) {
+    if (int s = check_batch(f, d_keys, n)) return s;
+    (void)d_out;
+    (void)stream;
+    (void)occupied_out;
+    return fail(CF_ERR_UNSUPPORTED, "insertManySorted is not built yet");
+}
+
+int cf_contains_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
+    if (int s = check_batch(f, d_keys, n)) return s;
+    if (n && !d_out) return fail(CF_ERR_INVALID, "d_out is NULL with n > 0");
+    DeviceGuard g(f->device);
+    CF_CUDA(f->ops->contains(dev(f), d_keys, n, d_out, launch(f, KID_CONTAINS, stream)), "contains launch");
+    return CF_OK;
+}
+
+int cf_contains(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
+    if (int s = cf_contains_async(f, d_keys, n, d_out, stream)) return s;
+    DeviceGuard g(f->device);
+    CF_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "stream synchronize");
+    return CF_OK;
+}
+
+int cf_delete_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
+    if (int s = check_batch(f, d_keys, n)) return s;
+    DeviceGuard g(f->device);
+    CF_CUDA(f->ops->remove(dev(f), d_keys, n, d_out, launch(f, KID_DELETE, stream)), "delete launch");
+    return CF_OK;
+}
+
+int cf_delete(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream, uint64_t* occupied_out) {
+    if (int s = cf_delete_async(f, d_keys, n, d_out, stream)) return s;
+    DeviceGuard g(f->device);
+    return finish(f, stream, occupied_out);
+}
+
+int cf_clear(cf_filter* f, void* stream) {
+    if (int s = check_filter(f)) return s;
+    DeviceGuard g(f->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CF_CUDA(cudaMemsetAsync(f->d_table, 0, f->table_bytes, s), "table clear");
+    CF_CUDA(cudaMemsetAsync(f->d_ctr, 0, CTR_COUNT * sizeof(unsigned long long), s), "counter clear");
+    CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    return CF_OK;
+}
+
+int cf_occupied(cf_filter* f, uint64_t* out) {
+    if (int s = check_filter(f)) return s;
+    if (!out) return fail(CF_ERR_INVALID, "out is NULL");
+    DeviceGuard g(f->device);
+    unsigned long long v = 0;
+    CF_CUDA(cudaMemcpy(&v, f->d_ctr + CTR_OCCUPIED, sizeof(v), cudaMemcpyDeviceToHost), "occupancy read");
+    *out = v;
+    return CF_OK;
+}
+
+int cf_count_occupied_slots(cf_filter* f, uint64_t* out) {
+    if (int s = check_filter(f)) return s;
+    if (!out) return fail(CF_ERR_INVALID, "out is NULL");
+    DeviceGuard g(f->device);
+    unsigned long long* d_res = nullptr;
+    CF_CUDA(cudaMalloc(&d_res, sizeof(unsigned long long)), "scratch allocation");
+    unsigned long long v = 0;
+    cudaError_t e = cudaMemset(d_res, 0, sizeof(v));
+    if (e == cudaSuccess) e = f->ops->count(dev(f), f->num_buckets, d_res, launch_aux(f, nullptr));
+    if (e == cudaSuccess) e = cudaMemcpy(&v, d_res, sizeof(v), cudaMemcpyDeviceToHost);
+    cudaFree(d_res);
+    CF_CUDA(e, "occupied-slot count");
+    *out = v;
+    return CF_OK;
+}
+
+int cf_get_stats(cf_filter* f, cf_stats* out) {
+    if (int s = check_filter(f)) return s;
+    if (!out) return fail(CF_ERR_INVALID, "out is NULL");
+    DeviceGuard g(f->device);
+    unsigned long long c[CTR_COUNT];
+    CF_CUDA(cudaMemcpy(c, f->d_ctr, sizeof(c), cudaMemcpyDeviceToHost), "counter read");
+    out->occupied = c[CTR_OCCUPIED];
+    out->primary = c[CTR_PRIMARY];
+    out->secondary = c[CTR_SECONDARY];
+    out->evicted_inserts = c[CTR_EVICTED_INSERTS];
+    out->evictions = c[CTR_EVICTIONS];
+    out->failed = c[CTR_FAILED];
+    out->lost = c[CTR_LOST];
+    out->removed = c[CTR_REMOVED];
+    return CF_OK;
+}
+
+int cf_reset_stats(cf_filter* f) {
+    if (int s = check_filter(f)) return s;
+    DeviceGuard g(f->device);
+    CF_CUDA(cudaMemset(f->d_ctr + 1, 0, (CTR_COUNT - 1) * sizeof(unsigned long long)), "counter reset");
+    return CF_OK;
+}
+
+int cf_table(cf_filter* f, void** d_table, uint64_t* bytes) {
+    if (int s = check_filter(f)) return s;
+    if (d_table) *d_table = f->d_table;
+    if (bytes) *bytes = f->table_bytes;
+    return CF_OK;
+}
+
+int cf_load_table(cf_filter* f, const void* src, uint64_t bytes, void* stream) {
+    if (int s = check_filter(f)) return s;
+    if (!src) return fail(CF_ERR_INVALID, "src is NULL");
+    if (bytes != f->table_bytes)
+        return fail(CF_ERR_INVALID, "image is %llu bytes, table is %llu", static_cast<unsigned long long>(bytes),
+                    static_cast<unsigned long long>(f->table_bytes));
+    DeviceGuard g(f->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CF_CUDA(cudaMemcpyAsync(f->d_table, src, bytes, cudaMemcpyDefault, s), "table load");
+    CF_CUDA(cudaMemsetAsync(f->d_ctr + CTR_OCCUPIED, 0, sizeof(unsigned long long), s), "counter reset");
+    CF_CUDA(f->ops->count(dev(f), f->num_buckets, f->d_ctr + CTR_OCCUPIED, launch_aux(f, stream)), "recount");
+    CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    return CF_OK;
+}
+
+int cf_store_table(cf_filter* f, void* dst, uint64_t bytes, void* stream) {
+    if (int s = check_filter(f)) return s;
+    if (!dst) return fail(CF_ERR_INVALID, "dst is NULL");
+    if (bytes != f->table_bytes)
+        return fail(CF_ERR_INVALID, "buffer is %llu bytes, table is %llu", static_cast<unsigned long long>(bytes),
+                    static_cast<unsigned long long>(f->table_bytes));
+    DeviceGuard g(f->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CF_CUDA(cudaMemcpyAsync(dst, f->d_table, bytes, cudaMemcpyDefault, s), "table store");
+    CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    return CF_OK;
+}
+
+int cf_hash_candidates(const cf_config* cfg, uint64_t num_buckets, const void* h_keys, uint64_t n, uint64_t* i1,
+                       uint64_t* i2, uint32_t* fp) {
+    if (!cfg) return fail(CF_ERR_INVALID, "config is NULL");
+    if (num_buckets == 0 || (num_buckets & (num_buckets - 1)))
+        return fail(CF_ERR_INVALID, "num_buckets must be a power of two");
+    if (n && !h_keys) return fail(CF_ERR_INVALID, "keys is NULL with n > 0");
+    const uint32_t kb = cfg->key_bytes, bits = cfg->bits_per_tag;
+    if ((kb != 4 && kb != 8) || (bits != 8 && bits != 16 && bits != 32))
+        return fail(CF_ERR_INVALID, "key_bytes must be 4/8 and bits_per_tag 8/16/32");
+    host_candidates(kb, bits, num_buckets - 1, h_keys, n, i1, i2, fp);
+    return CF_OK;
+}
+
+int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* primary_hits, void* stream) {
+    if (int s = check_batch(f, d_keys, n)) return s;
+    if (!primary_hits) return fail(CF_ERR_INVALID, "primary_hits is NULL");
+    DeviceGuard g(f->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned long long* d_res = nullptr;
+    CF_CUDA(cudaMalloc(&d_res, sizeof(unsigned long long)), "scratch allocation");
+    unsigned long long v = 0;
+    cudaError_t e = cudaMemsetAsync(d_res, 0, sizeof(v), s);
+    if (e == cudaSuccess) e = f->ops->probe(dev(f), d_keys, n, d_res, launch_aux(f, stream));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&v, d_res, sizeof(v), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_res);
+    CF_CUDA(e, "probe count");
+    *primary_hits = v;
+    return CF_OK;
+}
+
+}  // extern "C"

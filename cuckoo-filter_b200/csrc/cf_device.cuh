@@ -1,0 +1,242 @@
+// cf_device.cuh -- device primitives of the B200 cuckoo filter.
+//
+// Hashing and bucket derivation are bit-exact with the reference:
+//   xxHash64, seed 0, over the little-endian bytes of the value
+//     (reference include/hashutil.cuh:71-161; only the < 32-byte branch is
+//     reachable for 1/2/4/8-byte inputs, and each size is written out here as
+//     straight-line code);
+//   fingerprint = (uint32)(h >> 32) & tagMask, 0 -> 1; primary = (uint32)h & (nb-1);
+//   alternate  = bucket ^ (xxHash64(tag as TagType) & (nb-1))
+//     (include/bucket_policies.cuh:46-61, :72-74).
+// Table layout is the reference's (include/CuckooFilter.cuh:224-237): bucket b is
+// bucketBytes contiguous bytes at b*bucketBytes; slot s holds its tag at byte
+// offset s*(bits/8), packed little-endian into 64-bit words, 0 = empty.
+#pragma once
+
+#include <cstdint>
+
+namespace cfb {
+
+// ----------------------------------------------------------------- xxHash64
+
+constexpr uint64_t XP1 = 11400714785074694791ULL;
+constexpr uint64_t XP2 = 14029467366897019727ULL;
+constexpr uint64_t XP3 = 1609587929392839161ULL;
+constexpr uint64_t XP4 = 9650029242287828579ULL;
+constexpr uint64_t XP5 = 2870177450012600261ULL;
+
+__host__ __device__ __forceinline__ uint64_t rotl64(uint64_t x, int r) {
+    return (x << r) | (x >> (64 - r));
+}
+
+__host__ __device__ __forceinline__ uint64_t xxh_avalanche(uint64_t h) {
+    h ^= h >> 33;
+    h *= XP2;
+    h ^= h >> 29;
+    h *= XP3;
+    h ^= h >> 32;
+    return h;
+}
+
+// XXH64 of an 8-byte value: one 8-byte lane step, then the avalanche.
+__host__ __device__ __forceinline__ uint64_t xxh64_u64(uint64_t v) {
+    uint64_t h = XP5 + 8;
+    uint64_t k = rotl64(v * XP2, 31) * XP1;
+    h ^= k;
+    h = rotl64(h, 27) * XP1 + XP4;
+    return xxh_avalanche(h);
+}
+
+// XXH64 of a 4-byte value: the 4-byte step, then the avalanche.
+__host__ __device__ __forceinline__ uint64_t xxh64_u32(uint32_t v) {
+    uint64_t h = XP5 + 4;
+    h ^= static_cast<uint64_t>(v) * XP1;
+    h = rotl64(h, 23) * XP2 + XP3;
+    return xxh_avalanche(h);
+}
+
+// XXH64 of a 2-byte value: two single-byte steps (low byte first).
+__host__ __device__ __forceinline__ uint64_t xxh64_u16(uint32_t v) {
+    uint64_t h = XP5 + 2;
+    h ^= static_cast<uint64_t>(v & 0xFF) * XP5;
+    h = rotl64(h, 11) * XP1;
+    h ^= static_cast<uint64_t>((v >> 8) & 0xFF) * XP5;
+    h = rotl64(h, 11) * XP1;
+    return xxh_avalanche(h);
+}
+
+// XXH64 of a 1-byte value.
+__host__ __device__ __forceinline__ uint64_t xxh64_u8(uint32_t v) {
+    uint64_t h = XP5 + 1;
+    h ^= static_cast<uint64_t>(v & 0xFF) * XP5;
+    h = rotl64(h, 11) * XP1;
+    return xxh_avalanche(h);
+}
+
+template <int KEY_BYTES>
+__host__ __device__ __forceinline__ uint64_t hash_key(uint64_t key) {
+    if constexpr (KEY_BYTES == 8) {
+        return xxh64_u64(key);
+    } else {
+        return xxh64_u32(static_cast<uint32_t>(key));
+    }
+}
+
+template <int BITS>
+__host__ __device__ __forceinline__ uint64_t hash_tag(uint32_t tag) {
+    if constexpr (BITS == 8) {
+        return xxh64_u8(tag);
+    } else if constexpr (BITS == 16) {
+        return xxh64_u16(tag);
+    } else {
+        return xxh64_u32(tag);
+    }
+}
+
+// ------------------------------------------------------------ configuration
+
+// KB = key bytes (4/8), BITS = tag bits (8/16/32), BS = slots per bucket,
+// WB = CAS word bytes (8; the reference's WordType).
+template <int KB, int BITS, int BS, int WB>
+struct Cfg {
+    static constexpr int key_bytes = KB;
+    static constexpr int bits = BITS;
+    static constexpr int bs = BS;
+    static constexpr int word_bytes = WB;
+    static constexpr int bucket_bytes = BS * BITS / 8;
+    static constexpr int nchunks = bucket_bytes / 8;     // 64-bit chunks per bucket
+    static constexpr int lanes_per_chunk = 64 / BITS;    // tags per 64-bit chunk
+    static constexpr int tpw = WB * 8 / BITS;            // tags per CAS word
+    static constexpr int wc = BS / tpw;                  // CAS words per bucket
+    static constexpr uint32_t tag_mask = BITS == 32 ? 0xFFFFFFFFu : ((1u << BITS) - 1u);
+    static_assert(KB == 4 || KB == 8, "key must be 4 or 8 bytes");
+    static_assert(BITS == 8 || BITS == 16 || BITS == 32, "tag must be 8, 16 or 32 bits");
+    static_assert((BS & (BS - 1)) == 0, "bucket size must be a power of two");
+    static_assert(bucket_bytes >= 8 && bucket_bytes % 8 == 0, "bucket must be a whole number of 8-byte chunks");
+    static_assert(WB == 8, "64-bit CAS words");
+    static_assert(BS % tpw == 0, "bucket size must be a multiple of tags per word");
+    static_assert(BS <= 64, "at most 64 slots per bucket");
+    using Key = typename std::conditional<KB == 8, uint64_t, uint32_t>::type;
+};
+
+// Bucket derivation (XorAltBucketPolicy::getCandidateBuckets).
+template <class C>
+__host__ __device__ __forceinline__ void candidates(uint64_t key, uint64_t nb_mask, uint64_t& i1, uint32_t& fp) {
+    const uint64_t h = hash_key<C::key_bytes>(key);
+    uint32_t f = static_cast<uint32_t>(h >> 32) & C::tag_mask;
+    fp = f == 0 ? 1u : f;
+    i1 = static_cast<uint64_t>(static_cast<uint32_t>(h)) & nb_mask;
+}
+
+template <class C>
+__host__ __device__ __forceinline__ uint64_t alt_bucket(uint64_t b, uint32_t tag, uint64_t nb_mask) {
+    return b ^ (hash_tag<C::bits>(tag) & nb_mask);
+}
+
+// ------------------------------------------------------------------- SWAR
+
+// Exact per-lane "lane == 0" test: the top bit of each lane of the result is set
+// iff that lane is zero.  Unlike the borrow-based test, no lane above a zero
+// lane is flagged, so the flags can be used directly.
+template <int BITS>
+__device__ __forceinline__ uint64_t zero_lanes(uint64_t v) {
+    constexpr uint64_t lo7 = BITS == 8 ? 0x7F7F7F7F7F7F7F7FULL
+                           : BITS == 16 ? 0x7FFF7FFF7FFF7FFFULL
+                                        : 0x7FFFFFFF7FFFFFFFULL;
+    return ~(((v & lo7) + lo7) | v | lo7);
+}
+
+template <int BITS>
+__device__ __forceinline__ uint64_t replicate(uint32_t tag) {
+    if constexpr (BITS == 8) {
+        return static_cast<uint64_t>(tag) * 0x0101010101010101ULL;
+    } else if constexpr (BITS == 16) {
+        return static_cast<uint64_t>(tag) * 0x0001000100010001ULL;
+    } else {
+        return static_cast<uint64_t>(tag) * 0x0000000100000001ULL;
+    }
+}
+
+// Index of the lowest flagged lane of a zero_lanes() result (mask != 0).
+template <int BITS>
+__device__ __forceinline__ int lowest_lane(uint64_t mask) {
+    return (__ffsll(static_cast<long long>(mask)) - 1) / BITS;
+}
+
+// ------------------------------------------------------------------- loads
+
+// Read-only bucket load through the non-coherent path, no L1 allocation (the
+// table is not written while a lookup batch runs).
+template <int BYTES>
+__device__ __forceinline__ void load_nc(const void* p, uint64_t* c) {
+    if constexpr (BYTES == 8) {
+        asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(c[0]) : "l"(p));
+    } else if constexpr (BYTES == 16) {
+        asm volatile("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];" : "=l"(c[0]), "=l"(c[1]) : "l"(p));
+    } else {
+#pragma unroll
+        for (int i = 0; i < BYTES / 32; ++i) {
+            asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                         : "=l"(c[4 * i]), "=l"(c[4 * i + 1]), "=l"(c[4 * i + 2]), "=l"(c[4 * i + 3])
+                         : "l"(static_cast<const char*>(p) + 32 * i));
+        }
+    }
+}
+
+// Bucket load for read-modify-write paths: relaxed at GPU scope so the values
+// are at least as new as L2; they only seed compare-and-swap expectations.
+template <int BYTES>
+__device__ __forceinline__ void load_rlx(const void* p, uint64_t* c) {
+    if constexpr (BYTES == 8) {
+        asm volatile("ld.relaxed.gpu.global.L1::no_allocate.u64 %0, [%1];" : "=l"(c[0]) : "l"(p) : "memory");
+    } else if constexpr (BYTES == 16) {
+        asm volatile("ld.relaxed.gpu.global.L1::no_allocate.v2.u64 {%0,%1}, [%2];"
+                     : "=l"(c[0]), "=l"(c[1])
+                     : "l"(p)
+                     : "memory");
+    } else {
+#pragma unroll
+        for (int i = 0; i < BYTES / 32; ++i) {
+            asm volatile("ld.relaxed.gpu.global.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                         : "=l"(c[4 * i]), "=l"(c[4 * i + 1]), "=l"(c[4 * i + 2]), "=l"(c[4 * i + 3])
+                         : "l"(static_cast<const char*>(p) + 32 * i)
+                         : "memory");
+        }
+    }
+}
+
+__device__ __forceinline__ uint64_t load_word_rlx(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint64_t cas64(uint64_t* p, uint64_t expected, uint64_t desired) {
+    return atomicCAS(reinterpret_cast<unsigned long long*>(p), expected, desired);
+}
+
+// Streaming key loads (read once).
+__device__ __forceinline__ uint64_t ld_stream_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void ld_stream_v4u64(const uint64_t* p, uint64_t& a, uint64_t& b, uint64_t& c,
+                                                uint64_t& d) {
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
+                 : "l"(p));
+}
+__device__ __forceinline__ void ld_stream_v4u32(const uint32_t* p, uint32_t& a, uint32_t& b, uint32_t& c,
+                                                uint32_t& d) {
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
+                 : "l"(p));
+}
+
+}  // namespace cfb

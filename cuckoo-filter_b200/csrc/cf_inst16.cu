@@ -1,0 +1,17 @@
+// cf_inst16.cu -- kernel instantiations for 16-bit tags (64-bit CAS words).
+#include "cf_registry.cuh"
+
+namespace cfb {
+
+void register_bits16(std::vector<OpsTable>& v) {
+    v.push_back(Launchers<Cfg<8, 16, 4, 8>>::table());
+    v.push_back(Launchers<Cfg<4, 16, 4, 8>>::table());
+    v.push_back(Launchers<Cfg<8, 16, 8, 8>>::table());
+    v.push_back(Launchers<Cfg<4, 16, 8, 8>>::table());
+    v.push_back(Launchers<Cfg<8, 16, 16, 8>>::table());
+    v.push_back(Launchers<Cfg<4, 16, 16, 8>>::table());
+    v.push_back(Launchers<Cfg<8, 16, 32, 8>>::table());
+    v.push_back(Launchers<Cfg<4, 16, 32, 8>>::table());
+}
+
+}  // namespace cfb

@@ -1,0 +1,516 @@
+// cf_kernels.cuh -- batch kernels of the B200 cuckoo filter.
+//
+// One thread owns KPT consecutive keys of a tile; a persistent grid strides
+// over tiles.  A thread issues the KPT primary-bucket loads back to back, then
+// the KPT secondary-bucket loads for the keys that missed, so each thread keeps
+// several independent 32-byte sector requests in flight (the reference keeps
+// one key per thread, CuckooFilter.cuh:1119-1183).
+//
+// Semantics follow the reference's device code:
+//   contains : tag in bucket i1 or i2                         (CuckooFilter.cuh:1088-1098)
+//   remove   : clear the first matching slot of i1, else i2   (:805-848, :1106-1116)
+//   insert   : first empty slot of i1, else i2, else evict    (:859-904, :1029-1080)
+//   BFS      : copy a candidate to its alternate bucket, then swap fp in (:967-1018)
+//   DFS      : exchange walk of at most maxEvictions steps    (:917-954)
+// "First slot" means: scan CAS words circularly from word (tag & (bs-1)) / tagsPerWord,
+// lowest lane of a word first.
+//
+// Differences from the reference, all deliberate:
+//   * a DFS walk that runs out of evictions is undone step by step, so a failed
+//     insert leaves every previously stored tag in place (the reference drops the
+//     tag in hand, CuckooFilter.cuh:953, which makes an earlier key a false
+//     negative);
+//   * every compare-and-swap retry loop is bounded; hitting the bound sets an
+//     error flag that the host turns into a status code;
+//   * counters are accumulated per thread and flushed once per warp.
+#pragma once
+
+#include <cstdint>
+
+#include "cf_device.cuh"
+
+namespace cfb {
+
+// Hard cap on maxEvictions: the DFS undo log lives in a per-thread local array.
+constexpr uint32_t kMaxEvictionsCap = 512;
+// Bound on compare-and-swap retries of one bucket operation.
+constexpr int kCasRetryLimit = 1 << 16;
+
+// Device counter slots (64-bit each).
+enum Counter : int {
+    CTR_OCCUPIED = 0,
+    CTR_PRIMARY = 1,
+    CTR_SECONDARY = 2,
+    CTR_EVICTED_INSERTS = 3,
+    CTR_EVICTIONS = 4,
+    CTR_FAILED = 5,
+    CTR_LOST = 6,
+    CTR_ERROR = 7,
+    CTR_REMOVED = 8,
+    CTR_COUNT = 16
+};
+constexpr uint64_t ERR_CAS_LIMIT = 1;
+
+struct DevTable {
+    uint8_t* buckets;
+    uint64_t nb_mask;
+    unsigned long long* ctr;
+};
+
+template <class C>
+__device__ __forceinline__ uint64_t* bucket_words(const DevTable& t, uint64_t b) {
+    return reinterpret_cast<uint64_t*>(t.buckets + b * static_cast<uint64_t>(C::bucket_bytes));
+}
+
+// Select element w of a register array without dynamic indexing.
+template <int N>
+__device__ __forceinline__ uint64_t pick(const uint64_t (&c)[N], int w) {
+    uint64_t r = c[0];
+#pragma unroll
+    for (int j = 1; j < N; ++j) r = (j == w) ? c[j] : r;
+    return r;
+}
+template <int N>
+__device__ __forceinline__ void put(uint64_t (&c)[N], int w, uint64_t v) {
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+        if (j == w) c[j] = v;
+}
+
+// First word, in circular order from sw, whose bit is set in `words` (wc bits).
+template <int WC>
+__device__ __forceinline__ int first_word(uint32_t words, int sw) {
+    if constexpr (WC == 1) {
+        return 0;
+    } else {
+        const uint32_t full = (1u << WC) - 1u;
+        const uint32_t rot = ((words >> sw) | (words << (WC - sw))) & full;
+        return (sw + __ffs(rot) - 1) & (WC - 1);
+    }
+}
+
+// tryInsertAtBucket on a bucket whose current image is in c (refreshed on
+// compare-and-swap failure).  Returns true when fp was stored.
+template <class C>
+__device__ bool try_insert(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp, bool& err) {
+    const int sw = static_cast<int>((fp & (C::bs - 1)) / C::tpw);
+    for (int it = 0; it < kCasRetryLimit; ++it) {
+        uint32_t words = 0;
+#pragma unroll
+        for (int j = 0; j < C::nchunks; ++j) words |= (zero_lanes<C::bits>(c[j]) != 0 ? 1u : 0u) << j;
+        if (!words) return false;
+        const int w = first_word<C::wc>(words, sw);
+        const uint64_t cur = pick(c, w);
+        const int lane = lowest_lane<C::bits>(zero_lanes<C::bits>(cur));
+        const uint64_t desired = cur | (static_cast<uint64_t>(fp) << (lane * C::bits));
+        const uint64_t old = cas64(bw + w, cur, desired);
+        if (old == cur) return true;
+        put(c, w, old);
+    }
+    err = true;
+    return false;
+}
+
+// tryRemoveAtBucket: clear the first slot holding fp.
+template <class C>
+__device__ bool try_remove(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp, bool& err) {
+    const int sw = static_cast<int>((fp & (C::bs - 1)) / C::tpw);
+    const uint64_t rep = replicate<C::bits>(fp);
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    for (int it = 0; it < kCasRetryLimit; ++it) {
+        uint32_t words = 0;
+#pragma unroll
+        for (int j = 0; j < C::nchunks; ++j) words |= (zero_lanes<C::bits>(c[j] ^ rep) != 0 ? 1u : 0u) << j;
+        if (!words) return false;
+        const int w = first_word<C::wc>(words, sw);
+        const uint64_t cur = pick(c, w);
+        const int lane = lowest_lane<C::bits>(zero_lanes<C::bits>(cur ^ rep));
+        const uint64_t desired = cur & ~(lane_mask << (lane * C::bits));
+        const uint64_t old = cas64(bw + w, cur, desired);
+        if (old == cur) return true;
+        put(c, w, old);
+    }
+    err = true;
+    return false;
+}
+
+template <class C>
+__device__ __forceinline__ bool has_tag(const uint64_t (&c)[C::nchunks], uint32_t fp) {
+    const uint64_t rep = replicate<C::bits>(fp);
+    uint64_t any = 0;
+#pragma unroll
+    for (int j = 0; j < C::nchunks; ++j) any |= zero_lanes<C::bits>(c[j] ^ rep);
+    return any != 0;
+}
+
+// Atomically replace the tag in `slot`; returns the tag that was there.
+template <class C>
+__device__ uint32_t exchange_slot(uint64_t* bw, uint32_t slot, uint32_t v, bool& err) {
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    const int w = static_cast<int>(slot / C::tpw);
+    const int sh = static_cast<int>(slot % C::tpw) * C::bits;
+    uint64_t cur = load_word_rlx(bw + w);
+    for (int it = 0; it < kCasRetryLimit; ++it) {
+        const uint64_t desired = (cur & ~(lane_mask << sh)) | (static_cast<uint64_t>(v) << sh);
+        const uint64_t old = cas64(bw + w, cur, desired);
+        if (old == cur) return static_cast<uint32_t>((cur >> sh) & lane_mask);
+        cur = old;
+    }
+    err = true;
+    return v;  // treated as "slot already held v": nothing moved
+}
+
+struct EvictStats {
+    uint32_t evictions = 0;
+    uint32_t lost = 0;
+};
+
+// insertWithEvictionDFS with undo.  Returns true when fp is stored.
+template <class C>
+__device__ __noinline__ bool evict_dfs(DevTable t, uint32_t fp, uint64_t start, uint64_t other, uint32_t max_ev,
+                                       EvictStats& st, bool& err) {
+    uint8_t path[kMaxEvictionsCap];
+    uint32_t cur = fp;
+    uint64_t cb = start;
+    for (uint32_t e = 0; e < max_ev; ++e) {
+        const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(cur) + 7ull * e) & (C::bs - 1));
+        path[e] = static_cast<uint8_t>(slot);
+        const uint32_t victim = exchange_slot<C>(bucket_words<C>(t, cb), slot, cur, err);
+        if (err) return false;
+        ++st.evictions;
+        if (victim == 0) return true;  // a slot emptied concurrently took the tag
+        cur = victim;
+        cb = alt_bucket<C>(cb, victim, t.nb_mask);
+        uint64_t c[C::nchunks];
+        uint64_t* bw = bucket_words<C>(t, cb);
+        load_rlx<C::bucket_bytes>(bw, c);
+        if (try_insert<C>(bw, c, cur, err)) return true;
+        if (err) return false;
+    }
+    // Out of evictions: walk the chain back.  The held tag returns to the
+    // bucket it was taken from, alt(cb, held), at the logged slot.
+    for (uint32_t e = max_ev; e-- > 0;) {
+        cb = alt_bucket<C>(cb, cur, t.nb_mask);
+        cur = exchange_slot<C>(bucket_words<C>(t, cb), path[e], cur, err);
+        if (err) return false;
+        if (cur == 0) return true;
+    }
+    if (cur == fp && (cb == start || cb == other)) return false;  // table restored, fp not stored
+    // Another walk crossed ours: the tag now in hand belongs to a different
+    // key, and fp is stored.  Give the stray tag one more chance.
+    {
+        uint64_t c[C::nchunks];
+        uint64_t* bw = bucket_words<C>(t, cb);
+        load_rlx<C::bucket_bytes>(bw, c);
+        if (try_insert<C>(bw, c, cur, err)) return true;
+        const uint64_t ab = alt_bucket<C>(cb, cur, t.nb_mask);
+        bw = bucket_words<C>(t, ab);
+        load_rlx<C::bucket_bytes>(bw, c);
+        if (try_insert<C>(bw, c, cur, err)) return true;
+    }
+    ++st.lost;
+    return true;
+}
+
+// insertWithEvictionBFS: up to min(8, bs/2) candidates of the start bucket are
+// moved to their alternate bucket (copy first, then swap fp in, undo the copy
+// if the candidate moved meanwhile); then DFS.
+template <class C>
+__device__ __noinline__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, uint64_t other, uint32_t max_ev,
+                                       EvictStats& st, bool& err) {
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    constexpr uint32_t ncand = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
+    uint64_t* sbw = bucket_words<C>(t, start);
+    for (uint32_t i = 0; i < ncand; ++i) {
+        const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * i) & (C::bs - 1));
+        const int w = static_cast<int>(slot / C::tpw);
+        const int sh = static_cast<int>(slot % C::tpw) * C::bits;
+        uint64_t word = load_word_rlx(sbw + w);
+        const uint32_t cand = static_cast<uint32_t>((word >> sh) & lane_mask);
+        uint64_t c[C::nchunks];
+        if (cand == 0) {
+            load_rlx<C::bucket_bytes>(sbw, c);
+            if (try_insert<C>(sbw, c, fp, err)) return true;
+            if (err) return false;
+            continue;
+        }
+        const uint64_t ab = alt_bucket<C>(start, cand, t.nb_mask);
+        uint64_t* abw = bucket_words<C>(t, ab);
+        load_rlx<C::bucket_bytes>(abw, c);
+        if (try_insert<C>(abw, c, cand, err)) {
+            word = load_word_rlx(sbw + w);
+            if (((word >> sh) & lane_mask) == cand) {
+                const uint64_t desired = (word & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
+                if (cas64(sbw + w, word, desired) == word) {
+                    ++st.evictions;
+                    return true;
+                }
+            }
+            load_rlx<C::bucket_bytes>(abw, c);
+            try_remove<C>(abw, c, cand, err);
+        }
+        if (err) return false;
+    }
+    return evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+}
+
+// ------------------------------------------------------------ key loading
+
+template <class C, int KPT>
+__device__ __forceinline__ void load_keys(const typename C::Key* keys, uint64_t k0, uint64_t n, bool vec_ok,
+                                          uint64_t (&key)[KPT]) {
+    if (vec_ok && k0 + KPT <= n) {
+        if constexpr (C::key_bytes == 8 && KPT % 4 == 0) {
+#pragma unroll
+            for (int j = 0; j < KPT; j += 4)
+                ld_stream_v4u64(reinterpret_cast<const uint64_t*>(keys) + k0 + j, key[j], key[j + 1], key[j + 2],
+                                key[j + 3]);
+            return;
+        } else if constexpr (C::key_bytes == 8 && KPT == 2) {
+            asm volatile("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];"
+                         : "=l"(key[0]), "=l"(key[1])
+                         : "l"(reinterpret_cast<const uint64_t*>(keys) + k0));
+            return;
+        } else if constexpr (C::key_bytes == 4 && KPT % 4 == 0) {
+#pragma unroll
+            for (int j = 0; j < KPT; j += 4) {
+                uint32_t a, b, c, d;
+                ld_stream_v4u32(reinterpret_cast<const uint32_t*>(keys) + k0 + j, a, b, c, d);
+                key[j] = a;
+                key[j + 1] = b;
+                key[j + 2] = c;
+                key[j + 3] = d;
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        key[j] = 0;
+        if (k0 + j < n) {
+            if constexpr (C::key_bytes == 8)
+                key[j] = ld_stream_u64(reinterpret_cast<const uint64_t*>(keys) + k0 + j);
+            else
+                key[j] = ld_stream_u32(reinterpret_cast<const uint32_t*>(keys) + k0 + j);
+        }
+    }
+}
+
+// Store KPT result bytes (bit j of `bits` -> out[k0 + j]).  When the run of
+// KPT bytes is aligned, one 1/2/4/8-byte streaming store writes them all.
+template <int KPT>
+__device__ __forceinline__ void store_results(uint8_t* out, uint64_t k0, uint64_t n, bool vec_ok, uint32_t bits) {
+    if (vec_ok && k0 + KPT <= n) {
+        uint64_t v = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) v |= static_cast<uint64_t>((bits >> j) & 1u) << (8 * j);
+        if constexpr (KPT == 8) {
+            asm volatile("st.global.cs.u64 [%0], %1;" ::"l"(out + k0), "l"(v) : "memory");
+        } else if constexpr (KPT == 4) {
+            asm volatile("st.global.cs.u32 [%0], %1;" ::"l"(out + k0), "r"(static_cast<uint32_t>(v)) : "memory");
+        } else if constexpr (KPT == 2) {
+            asm volatile("st.global.cs.u16 [%0], %1;" ::"l"(out + k0), "h"(static_cast<uint16_t>(v)) : "memory");
+        } else {
+            out[k0] = static_cast<uint8_t>(v);
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < KPT; ++j)
+        if (k0 + j < n) out[k0 + j] = static_cast<uint8_t>((bits >> j) & 1u);
+}
+
+__device__ __forceinline__ void flush_counter(unsigned long long* ctr, uint32_t v) {
+    const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(ctr, static_cast<unsigned long long>(s));
+}
+
+// ------------------------------------------------------------------ kernels
+
+template <class C, int KPT>
+__global__ void __launch_bounds__(512) k_contains(DevTable t, const typename C::Key* __restrict__ keys, uint64_t n,
+                                                  uint8_t* __restrict__ out, bool keys_vec, bool out_vec) {
+    const uint64_t tile = static_cast<uint64_t>(blockDim.x) * KPT;
+    for (uint64_t base = blockIdx.x * tile; base < n; base += static_cast<uint64_t>(gridDim.x) * tile) {
+        const uint64_t k0 = base + static_cast<uint64_t>(threadIdx.x) * KPT;
+        if (k0 >= n) continue;
+        uint64_t key[KPT];
+        load_keys<C, KPT>(keys, k0, n, keys_vec, key);
+        uint64_t b[KPT];
+        uint32_t fp[KPT];
+        uint64_t c[KPT][C::nchunks];
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            candidates<C>(key[j], t.nb_mask, b[j], fp[j]);
+            if (k0 + j < n) load_nc<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
+        }
+        uint32_t hit = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+            if (k0 + j < n && has_tag<C>(c[j], fp[j])) hit |= 1u << j;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            if (k0 + j < n && !((hit >> j) & 1u)) {
+                b[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
+                load_nc<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+            if (k0 + j < n && !((hit >> j) & 1u) && has_tag<C>(c[j], fp[j])) hit |= 1u << j;
+        store_results<KPT>(out, k0, n, out_vec, hit);
+    }
+}
+
+template <class C, int KPT>
+__global__ void __launch_bounds__(512) k_delete(DevTable t, const typename C::Key* __restrict__ keys, uint64_t n,
+                                                uint8_t* __restrict__ out, bool keys_vec, bool out_vec) {
+    const uint64_t tile = static_cast<uint64_t>(blockDim.x) * KPT;
+    uint32_t removed = 0;
+    bool err = false;
+    for (uint64_t base = blockIdx.x * tile; base < n; base += static_cast<uint64_t>(gridDim.x) * tile) {
+        const uint64_t k0 = base + static_cast<uint64_t>(threadIdx.x) * KPT;
+        if (k0 >= n) continue;
+        uint64_t key[KPT];
+        load_keys<C, KPT>(keys, k0, n, keys_vec, key);
+        uint64_t b[KPT];
+        uint32_t fp[KPT];
+        uint64_t c[KPT][C::nchunks];
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            candidates<C>(key[j], t.nb_mask, b[j], fp[j]);
+            if (k0 + j < n) load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
+        }
+        uint32_t done = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+            if (k0 + j < n && try_remove<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err)) done |= 1u << j;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            if (k0 + j < n && !((done >> j) & 1u)) {
+                b[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
+                load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+            if (k0 + j < n && !((done >> j) & 1u) && try_remove<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err))
+                done |= 1u << j;
+        removed += __popc(done);
+        if (out) store_results<KPT>(out, k0, n, out_vec, done);
+    }
+    const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, removed);
+    if ((threadIdx.x & 31) == 0 && s) {
+        atomicAdd(&t.ctr[CTR_REMOVED], static_cast<unsigned long long>(s));
+        atomicAdd(&t.ctr[CTR_OCCUPIED], ~static_cast<unsigned long long>(s) + 1ull);  // -= s
+    }
+    if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+template <class C, int KPT>
+__global__ void __launch_bounds__(512) k_insert(DevTable t, const typename C::Key* __restrict__ keys, uint64_t n,
+                                                uint8_t* __restrict__ out, bool keys_vec, bool out_vec,
+                                                uint32_t policy_bfs, uint32_t max_ev) {
+    const uint64_t tile = static_cast<uint64_t>(blockDim.x) * KPT;
+    uint32_t n_prim = 0, n_sec = 0, n_evk = 0, n_fail = 0;
+    EvictStats st;
+    bool err = false;
+    for (uint64_t base = blockIdx.x * tile; base < n; base += static_cast<uint64_t>(gridDim.x) * tile) {
+        const uint64_t k0 = base + static_cast<uint64_t>(threadIdx.x) * KPT;
+        if (k0 >= n) continue;
+        uint64_t key[KPT];
+        load_keys<C, KPT>(keys, k0, n, keys_vec, key);
+        uint64_t b[KPT];
+        uint32_t fp[KPT];
+        uint64_t c[KPT][C::nchunks];
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            candidates<C>(key[j], t.nb_mask, b[j], fp[j]);
+            if (k0 + j < n) load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
+        }
+        uint32_t done = 0, valid = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            if (k0 + j < n) {
+                valid |= 1u << j;
+                if (try_insert<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err)) done |= 1u << j;
+            }
+        }
+        n_prim += __popc(done);
+        uint64_t b2[KPT];
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            b2[j] = 0;
+            if (((valid & ~done) >> j) & 1u) {
+                b2[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
+                load_rlx<C::bucket_bytes>(t.buckets + b2[j] * C::bucket_bytes, c[j]);
+            }
+        }
+        uint32_t sec = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+            if (((valid & ~done) >> j) & 1u && try_insert<C>(bucket_words<C>(t, b2[j]), c[j], fp[j], err))
+                sec |= 1u << j;
+        n_sec += __popc(sec);
+        done |= sec;
+        const uint32_t hard = valid & ~done;
+        if (hard) {
+#pragma unroll 1
+            for (int j = 0; j < KPT; ++j) {
+                if (!((hard >> j) & 1u)) continue;
+                ++n_evk;
+                const uint64_t start = (fp[j] & 1u) == 0 ? b[j] : b2[j];
+                const uint64_t other = (fp[j] & 1u) == 0 ? b2[j] : b[j];
+                const bool ok = policy_bfs ? evict_bfs<C>(t, fp[j], start, other, max_ev, st, err)
+                                           : evict_dfs<C>(t, fp[j], start, other, max_ev, st, err);
+                if (ok)
+                    done |= 1u << j;
+                else
+                    ++n_fail;
+            }
+        }
+        if (out) store_results<KPT>(out, k0, n, out_vec, done);
+    }
+    flush_counter(&t.ctr[CTR_OCCUPIED], n_prim + n_sec + (n_evk - n_fail));
+    flush_counter(&t.ctr[CTR_PRIMARY], n_prim);
+    flush_counter(&t.ctr[CTR_SECONDARY], n_sec);
+    flush_counter(&t.ctr[CTR_EVICTED_INSERTS], n_evk);
+    flush_counter(&t.ctr[CTR_EVICTIONS], st.evictions);
+    flush_counter(&t.ctr[CTR_FAILED], n_fail);
+    flush_counter(&t.ctr[CTR_LOST], st.lost);
+    if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// Occupied-slot count of the whole table (countOccupiedSlots, CuckooFilter.cuh:759-785).
+template <class C>
+__global__ void k_count_occupied(DevTable t, uint64_t nb, unsigned long long* result) {
+    uint32_t cnt = 0;
+    for (uint64_t b = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; b < nb;
+         b += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t c[C::nchunks];
+        load_nc<C::bucket_bytes>(t.buckets + b * C::bucket_bytes, c);
+#pragma unroll
+        for (int j = 0; j < C::nchunks; ++j) cnt += C::lanes_per_chunk - __popcll(zero_lanes<C::bits>(c[j]));
+    }
+    flush_counter(result, cnt);
+}
+
+// Probe accounting for the roofline: how many lookups of this batch find their
+// tag in the primary bucket (1 sector) versus need the secondary (2 sectors).
+template <class C>
+__global__ void k_probe_count(DevTable t, const typename C::Key* __restrict__ keys, uint64_t n,
+                              unsigned long long* result) {
+    uint32_t prim = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t b;
+        uint32_t fp;
+        candidates<C>(static_cast<uint64_t>(keys[i]), t.nb_mask, b, fp);
+        uint64_t c[C::nchunks];
+        load_nc<C::bucket_bytes>(t.buckets + b * C::bucket_bytes, c);
+        prim += has_tag<C>(c, fp) ? 1u : 0u;
+    }
+    flush_counter(result, prim);
+}
+
+}  // namespace cfb

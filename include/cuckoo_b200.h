@@ -1,0 +1,190 @@
+/*
+ * cuckoo_b200.h -- C ABI of the B200 cuckoo filter (libcuckoo_b200.so).
+ *
+ * This is the drop-in boundary for the batch path of the reference's
+ * header-only CuckooFilter<Config> (reference include/CuckooFilter.cuh).  Every
+ * entry point takes plain pointers and sizes; device pointers are CUDA device
+ * (or managed) memory on the device the filter was created on; `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).
+ *
+ * All functions return CF_OK (0) or a negative cf_status; on error a message is
+ * available from cf_last_error() on the calling thread.  Nothing here exits the
+ * process (the reference's CUDA_CALL prints and calls exit(), helpers.cuh:202-210).
+ *
+ * Table image: identical to the reference's (CuckooFilter.cuh:224-237): bucket b
+ * is bucket_bytes = bucket_size*bits_per_tag/8 contiguous bytes at offset
+ * b*bucket_bytes; slot s holds its tag at byte s*bits_per_tag/8 of the bucket,
+ * 0 means empty.  num_buckets is a power of two.
+ */
+#ifndef CUCKOO_B200_H
+#define CUCKOO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CF_ABI_VERSION 1
+
+typedef enum cf_status {
+    CF_OK = 0,
+    CF_ERR_INVALID = -1,     /* bad argument or configuration */
+    CF_ERR_UNSUPPORTED = -2, /* configuration not compiled into this library */
+    CF_ERR_CUDA = -3,        /* CUDA runtime error (see cf_last_error) */
+    CF_ERR_NO_MEMORY = -4,   /* device or pinned allocation failed */
+    CF_ERR_DEVICE = -5,      /* a device-side retry bound was hit; table is consistent */
+    CF_ERR_NOT_LOADED = -6   /* no usable CUDA device */
+} cf_status;
+
+/* Eviction policy (reference enum class EvictionPolicy, CuckooFilter.cuh:19-22). */
+typedef enum cf_eviction { CF_EVICT_BFS = 0, CF_EVICT_DFS = 1 } cf_eviction;
+
+/* Alternate-bucket policy (reference bucket_policies.cuh).  Only the XOR policy
+ * (XorAltBucketPolicy, :15-84) is implemented. */
+typedef enum cf_alt_policy { CF_ALT_XOR = 0 } cf_alt_policy;
+
+/*
+ * Runtime form of CuckooConfig<T, bitsPerTag, maxEvictions, blockSize,
+ * bucketSize, AltBucketPolicy, evictionPolicy, WordType>
+ * (reference include/CuckooFilter.cuh:44-74).
+ */
+typedef struct cf_config {
+    uint32_t key_bytes;       /* sizeof(T): 4 (uint32_t) or 8 (uint64_t) */
+    uint32_t bits_per_tag;    /* bitsPerTag: 8, 16 or 32 */
+    uint32_t bucket_size;     /* bucketSize: slots per bucket, power of two, 8..64 bytes per bucket */
+    uint32_t word_bytes;      /* sizeof(WordType): 8 */
+    uint32_t eviction_policy; /* cf_eviction */
+    uint32_t max_evictions;   /* maxEvictions: 1..512 */
+    uint32_t block_size;      /* blockSize: threads per block, multiple of 32, <= 512; 0 = tuned */
+    uint32_t alt_policy;      /* cf_alt_policy */
+} cf_config;
+
+typedef struct cf_filter cf_filter;
+
+/* Geometry of a created filter. */
+typedef struct cf_info {
+    uint64_t num_buckets;   /* getNumBuckets() (CuckooFilter.cuh:740) */
+    uint64_t capacity;      /* capacity() = num_buckets * bucket_size (:732) */
+    uint64_t size_in_bytes; /* sizeInBytes() = num_buckets * bucket_bytes (:748) */
+    uint32_t bucket_bytes;
+    int32_t device;
+} cf_info;
+
+/* Cumulative device counters since creation or cf_reset_stats(). */
+typedef struct cf_stats {
+    uint64_t occupied;        /* occupiedSlots() (:699-704) */
+    uint64_t primary;         /* inserts stored in their primary bucket */
+    uint64_t secondary;       /* inserts stored in their alternate bucket */
+    uint64_t evicted_inserts; /* inserts that needed eviction */
+    uint64_t evictions;       /* slot exchanges performed (the reference's evictionCount(), :714) */
+    uint64_t failed;          /* inserts that failed (table unchanged for that key) */
+    uint64_t lost;            /* stored tags dropped by crossing eviction walks (expected 0) */
+    uint64_t removed;         /* successful deletes */
+} cf_stats;
+
+/* Library ABI version (CF_ABI_VERSION). */
+int cf_abi_version(void);
+
+/* Message for the last failed call on this thread ("" if none). */
+const char* cf_last_error(void);
+
+/* Name of a status code. */
+const char* cf_status_string(int status);
+
+/* 1 if (key_bytes, bits_per_tag, bucket_size, word_bytes) is compiled in. */
+int cf_config_supported(const cf_config* cfg);
+
+/* Number of buckets the filter would use for `capacity` slots:
+ * nextPowerOfTwo(ceil(capacity / bucket_size)) (XorAltBucketPolicy::calculateNumBuckets,
+ * bucket_policies.cuh:80-83). */
+uint64_t cf_num_buckets_for(uint64_t capacity, uint32_t bucket_size);
+
+/* explicit CuckooFilter(size_t capacity) (CuckooFilter.cuh:420-428): allocates
+ * and zeroes the table on the current device. */
+int cf_create(const cf_config* cfg, uint64_t capacity, cf_filter** out);
+
+/* ~CuckooFilter() (CuckooFilter.cuh:435-447). NULL is accepted. */
+int cf_destroy(cf_filter* f);
+
+int cf_get_info(const cf_filter* f, cf_info* out);
+
+/*
+ * size_t insertMany(const T* d_keys, size_t n, cudaStream_t) (CuckooFilter.cuh:457-464).
+ * Synchronous on `stream`; *occupied_out (optional) receives occupiedSlots()
+ * after the batch.  d_out (optional, n bytes) receives 1 for each key stored,
+ * 0 for each key whose insert failed (extension: the reference reports only the
+ * count).  A failed insert leaves every previously stored tag in place.
+ */
+int cf_insert(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,
+              uint64_t* occupied_out);
+
+/*
+ * size_t insertManySorted(const T* d_keys, size_t n, cudaStream_t)
+ * (CuckooFilter.cuh:475-508).  Same contract as cf_insert; keys are first
+ * partitioned by primary bucket so that table writes are coalesced.
+ */
+int cf_insert_sorted(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,
+                     uint64_t* occupied_out);
+
+/*
+ * void containsMany(const T* d_keys, size_t n, bool* d_output, cudaStream_t)
+ * (CuckooFilter.cuh:518-523).  d_out: n bytes, 1 = maybe present, 0 = absent.
+ * Synchronous on `stream`.
+ */
+int cf_contains(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream);
+
+/*
+ * size_t deleteMany(const T* d_keys, size_t n, bool* d_output, cudaStream_t)
+ * (CuckooFilter.cuh:536-548).  Removes one copy per key; d_out (optional)
+ * receives 1 per removed key.  Synchronous; *occupied_out (optional) as above.
+ */
+int cf_delete(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,
+              uint64_t* occupied_out);
+
+/* Asynchronous forms: enqueue on `stream` and return; counters stay on the
+ * device (read them with cf_occupied / cf_get_stats, which synchronize). */
+int cf_insert_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream);
+int cf_contains_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream);
+int cf_delete_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream);
+
+/* void clear() (CuckooFilter.cuh:675-682): zero the table and the counters. */
+int cf_clear(cf_filter* f, void* stream);
+
+/* size_t occupiedSlots() (CuckooFilter.cuh:699-704). Synchronizes the device. */
+int cf_occupied(cf_filter* f, uint64_t* out);
+
+/* size_t countOccupiedSlots() (CuckooFilter.cuh:759-785): counts non-empty
+ * slots of the table image (on the device). */
+int cf_count_occupied_slots(cf_filter* f, uint64_t* out);
+
+int cf_get_stats(cf_filter* f, cf_stats* out);
+/* Zero all counters except `occupied` (resetEvictionCount(), CuckooFilter.cuh:723). */
+int cf_reset_stats(cf_filter* f);
+
+/* Device pointer to the table image and its size (the reference's d_buckets, :350). */
+int cf_table(cf_filter* f, void** d_table, uint64_t* bytes);
+
+/* Replace the table image with `bytes` bytes from `src` (device or host memory)
+ * and recount the occupancy.  Synchronous. */
+int cf_load_table(cf_filter* f, const void* src, uint64_t bytes, void* stream);
+
+/* Copy the table image to `dst` (device or host memory, `bytes` == table size). Synchronous. */
+int cf_store_table(cf_filter* f, void* dst, uint64_t bytes, void* stream);
+
+/* static getCandidateBuckets(key, numBuckets) (CuckooFilter.cuh:366-369 ->
+ * XorAltBucketPolicy::getCandidateBuckets, bucket_policies.cuh:46-61) for n
+ * HOST keys: the kernels' hashing evaluated on the CPU.  Any of i1/i2/fp may be NULL. */
+int cf_hash_candidates(const cf_config* cfg, uint64_t num_buckets, const void* h_keys, uint64_t n, uint64_t* i1,
+                       uint64_t* i2, uint32_t* fp);
+
+/* Lookups of this batch whose tag is in the primary bucket (one probe); the
+ * rest take two probes.  Diagnostic for sector accounting. */
+int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* primary_hits, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUCKOO_B200_H */

@@ -1,0 +1,56 @@
+"""Host logic of bench.py: key generators and disjointness (CPU only)."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+import bench
+
+
+def test_torch_splitmix64_matches_oracle(orc):
+    for seed, first, n in ((3, 0, 1000), (4, 12345, 777), (1, 0, 1 << 16)):
+        t = torch.empty(n, dtype=torch.int64)
+        bench.splitmix64_torch(seed, first, n, t, chunk=4096)
+        assert np.array_equal(t.numpy().view(np.uint64), orc.splitmix64(seed, n, first))
+
+
+def test_negative_collisions_exact():
+    # seed_neg = seed_pos + 5*gamma: negative j equals positive j + 5
+    sp = 3
+    sn = (sp + 5 * bench.G) % bench.U64
+    bad = bench.negative_collisions(sp, 100, sn, 200)
+    assert bad == list(range(0, 95))
+    assert bench.collides(sp, 100, sn, 94) and not bench.collides(sp, 100, sn, 95)
+    # the default seeds of the workloads do not collide
+    for w in bench.WORKLOADS.values():
+        n_fill = int(w["fill"] * w["capacity"])
+        assert bench.negative_collisions(w["seed_fill"], n_fill, w["seed_neg"], w["n_neg"]) == []
+
+
+def test_negative_collisions_against_brute_force(orc):
+    sp, sn = 11, (11 + 1000 * bench.G) % bench.U64
+    pos = orc.splitmix64(sp, 3000)
+    neg = orc.splitmix64(sn, 3000)
+    brute = [j for j in range(3000) if neg[j] in set(pos.tolist())]
+    assert bench.negative_collisions(sp, 3000, sn, 3000) == brute
+
+
+def test_small_workload_inputs_cpu():
+    w = dict(bench.WORKLOADS["small"])
+    fill, query, dele, n_coll = bench.make_inputs(w, torch.device("cpu"))
+    assert n_coll == 0
+    assert fill.numel() == int(0.95 * (1 << 20)) == 996147
+    assert query.numel() == 2 * 996147 and dele.numel() == 996147 // 2
+    assert torch.unique(fill).numel() == fill.numel()
+    pos = set(fill.tolist())
+    q = query.tolist()
+    assert sum(1 for x in q if x in pos) == 996147
+    assert all(x in pos for x in dele.tolist())
+
+
+def test_positive_sample_without_replacement():
+    w = dict(bench.WORKLOADS["small"], capacity=1 << 16, n_pos=20000, n_neg=20000, n_del=5000, seed_sample=9)
+    fill, query, dele, _ = bench.make_inputs(w, torch.device("cpu"))
+    pos = set(fill.tolist())
+    qp = [x for x in query.tolist() if x in pos]
+    assert len(qp) == 20000 == len(set(qp))

@@ -1,0 +1,364 @@
+"""Parity of the CUDA path with the oracle and with the reference's own kernels.
+
+All calls go through the C ABI (``cuckoo_b200`` -> libcuckoo_b200.so).
+
+Exact (bit-for-bit) checks:
+  * one-key-at-a-time inserts produce the oracle's table image (conserving
+    mode), evictions and failed chains included; the reference's own kernels run
+    the same way produce the oracle's reference-mode image up to the first
+    failed chain;
+  * containsMany on an identical table image equals the oracle and the
+    reference's containsMany;
+  * deleteMany one key at a time equals the oracle.
+Concurrent batches (not deterministic) are checked through invariants: zero
+false negatives, the table's (bucket pair, tag) multiset equals the stored
+keys', counters agree with the image, failure counts and false-positive rates
+within 3 sigma of the oracle's on the same keys.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(a: np.ndarray):
+    if a.dtype == np.uint64:
+        a = a.view(np.int64)
+    elif a.dtype == np.uint32:
+        a = a.view(np.int32)
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host_u8(t) -> np.ndarray:
+    return t.to(torch.uint8).cpu().numpy()
+
+
+def make(cfb, orc, key_bytes=8, bits=16, bs=16, policy=1, max_ev=500, capacity=1 << 12):
+    cfg = cfb.CuckooConfig(T="uint64" if key_bytes == 8 else "uint32", bitsPerTag=bits, bucketSize=bs,
+                           maxEvictions=max_ev, evictionPolicy=cfb.EvictionPolicy(policy))
+    f = cfb.CuckooFilter(cfg, capacity)
+    o = orc.OracleFilter(key_bytes=key_bytes, bits=bits, bucket_size=bs, policy=policy, max_evictions=max_ev,
+                         capacity=capacity, mode=orc.MODE_CONSERVING)
+    assert f.getNumBuckets() == o.nb
+    return f, o
+
+
+def image(f) -> np.ndarray:
+    return f.table_image(device="cpu").numpy()
+
+
+def alt_fn(orc, o):
+    if o.bits <= 16:
+        return orc.alt_vectorized(o.bits, o.nb)
+    return lambda b, t: np.array([o.alt_bucket(int(x), int(y)) for x, y in zip(b, t)], dtype=np.uint64)
+
+
+SEQ_CASES = [
+    # key_bytes, bits, bs, policy, max_ev, capacity, fill
+    (8, 16, 16, 0, 500, 1 << 12, 0.97),
+    (8, 16, 16, 1, 500, 1 << 12, 0.97),
+    (8, 16, 16, 1, 16, 1 << 12, 1.00),
+    (8, 8, 16, 0, 500, 1 << 12, 0.97),
+    (8, 32, 8, 1, 16, 1 << 11, 1.00),
+    (8, 32, 8, 0, 16, 1 << 11, 1.00),
+    (4, 16, 16, 1, 500, 1 << 12, 0.97),
+    (8, 16, 4, 0, 32, 1 << 10, 1.00),
+    (8, 8, 64, 1, 64, 1 << 12, 0.99),
+]
+
+
+@pytest.mark.parametrize("kb,bits,bs,policy,max_ev,cap,fill", SEQ_CASES)
+def test_sequential_image_bit_exact(cfb, orc, kb, bits, bs, policy, max_ev, cap, fill):
+    f, o = make(cfb, orc, kb, bits, bs, policy, max_ev, cap)
+    keys = orc.splitmix64(100 + bits + bs + policy, int(fill * f.capacity()))
+    if kb == 4:
+        keys = keys.astype(np.uint32)
+    d = dev(keys)
+    out = torch.empty(1, dtype=torch.bool, device="cuda")
+    got = np.empty(len(keys), np.uint8)
+    for i in range(len(keys)):
+        f.insertMany(d[i:i + 1], d_output=out)
+        got[i] = int(out.item())
+    n_ok, want = o.insert(keys, out=True)
+    assert np.array_equal(got, want), f"first differing key {int(np.argmax(got != want))}"
+    assert np.array_equal(image(f), o.table)
+    st = f.stats()
+    assert st["occupied"] == n_ok == f.countOccupiedSlots()
+    assert st["lost"] == 0
+    assert st["failed"] == len(keys) - n_ok
+    if fill >= 1.0:
+        assert st["failed"] > 0, "case meant to exercise failed chains"
+    assert st["evictions"] > 0
+
+
+@pytest.mark.parametrize("cfg_key,cap", [((8, 16, 16, 0, 500), 1 << 12), ((8, 16, 16, 1, 16), 1 << 12),
+                                         ((8, 32, 8, 1, 16), 1 << 11), ((8, 32, 8, 0, 16), 1 << 11),
+                                         ((8, 8, 16, 1, 500), 1 << 12)])
+def test_reference_kernels_sequential_image_matches_oracle(cfb, orc, cfg_key, cap):
+    """The reference's own CUDA kernels, one key per launch, against the oracle's
+    reference mode (drop-on-failure) up to the first failed chain."""
+    if orc.ref_gpu() is None:
+        pytest.skip("oracle/_ref/libref_gpu.so not built")
+    kb, bits, bs, policy, max_ev = cfg_key
+    ref = orc.RefGpuFilter(kb, bits, bs, policy, max_ev, cap)
+    try:
+        o = orc.OracleFilter(key_bytes=kb, bits=bits, bucket_size=bs, policy=policy, max_evictions=max_ev,
+                             capacity=cap, mode=orc.MODE_REFERENCE)
+        assert ref.num_buckets() == o.nb
+        keys = orc.splitmix64(300 + bits + policy, cap)
+        d = dev(keys)
+        prev = 0
+        for i in range(len(keys)):
+            occ = ref.insert(d[i:i + 1].data_ptr(), 1)
+            ok = occ - prev
+            prev = occ
+            want = o.insert(keys[i:i + 1])
+            assert ok == want, i
+            if want == 0 or i == len(keys) - 1 or i % 512 == 0:
+                assert np.array_equal(_ref_image(cfb, ref, kb, bits, bs), o.table), f"image differs after key {i}"
+            if want == 0:
+                break
+    finally:
+        ref.close()
+
+
+def _ref_image(cfb, ref, kb, bits, bs) -> np.ndarray:
+    """Host copy of the reference filter's table, read through a scratch filter
+    of the same geometry (cf_load_table copies from any device pointer)."""
+    ptr, nbytes = ref.table()
+    cfg = cfb.CuckooConfig(T="uint64" if kb == 8 else "uint32", bitsPerTag=bits, bucketSize=bs)
+    scratch = cfb.CuckooFilter(cfg, ref.num_buckets() * bs)
+    try:
+        scratch.load_table(ptr, nbytes)
+        return image(scratch)
+    finally:
+        scratch.close()
+
+
+LOOKUP_CASES = [(8, 16, 16), (8, 8, 16), (8, 32, 8), (4, 16, 16), (8, 16, 4), (8, 8, 64), (8, 16, 32), (4, 32, 16)]
+
+
+@pytest.mark.parametrize("kb,bits,bs", LOOKUP_CASES)
+def test_contains_on_identical_image(cfb, orc, kb, bits, bs):
+    cap = 1 << 16
+    f, o = make(cfb, orc, kb, bits, bs, 0, 500, cap)
+    pos = orc.splitmix64(1, int(0.93 * f.capacity()))
+    neg = orc.splitmix64(2, 200_000)
+    if kb == 4:
+        pos, neg = pos.astype(np.uint32), neg.astype(np.uint32)
+    o.insert(pos)
+    f.load_table(torch.from_numpy(o.table).cuda())
+    assert f.occupiedSlots() == o.occupied()
+    q = np.concatenate([pos, neg])
+    got = host_u8(f.containsMany(dev(q)))
+    want = o.contains(q, threads=4)
+    assert np.array_equal(got, want)
+    assert got[: len(pos)].all()
+    assert f.probe_count(dev(q)) == 2 * len(q) - o.probe_count(q)
+
+
+@pytest.mark.parametrize("cfg_key", [(8, 16, 16, 0, 500), (8, 8, 16, 1, 500), (8, 32, 8, 0, 500), (4, 16, 16, 1, 500)])
+def test_contains_matches_reference_kernels_on_identical_image(cfb, orc, cfg_key):
+    if orc.ref_gpu() is None:
+        pytest.skip("oracle/_ref/libref_gpu.so not built")
+    kb, bits, bs, policy, max_ev = cfg_key
+    cap = 1 << 18
+    f, o = make(cfb, orc, kb, bits, bs, policy, max_ev, cap)
+    pos = orc.splitmix64(31, int(0.95 * f.capacity()))
+    neg = orc.splitmix64(32, 300_000)
+    if kb == 4:
+        pos, neg = pos.astype(np.uint32), neg.astype(np.uint32)
+    d_pos = dev(pos)
+    f.insertMany(d_pos)
+    ref = orc.RefGpuFilter(kb, bits, bs, policy, max_ev, cap)
+    try:
+        ptr, nbytes = ref.table()
+        assert nbytes == f.sizeInBytes()
+        f.store_table(ptr, nbytes)  # identical image in the reference's d_buckets
+        q = dev(np.concatenate([pos, neg]))
+        ref_out = torch.zeros(q.numel(), dtype=torch.uint8, device="cuda")
+        ref.contains(q.data_ptr(), q.numel(), ref_out.data_ptr())
+        mine = f.containsMany(q)
+        assert torch.equal(mine.to(torch.uint8), ref_out)
+    finally:
+        ref.close()
+
+
+def _stored_invariants(f, o, orc, stored_keys):
+    slots = image(f).view({8: np.uint8, 16: np.uint16, 32: np.uint32}[o.bits]).reshape(o.nb, o.bucket_size)
+    i1, i2, fp = o.candidates(stored_keys)
+    return orc.check_invariants(slots, alt_fn(orc, o), i1, i2, fp)
+
+
+BULK_CASES = [(8, 16, 16, 0), (8, 16, 16, 1), (8, 8, 16, 0), (8, 32, 8, 1), (8, 32, 8, 0), (4, 16, 16, 1)]
+
+
+@pytest.mark.parametrize("kb,bits,bs,policy", BULK_CASES)
+def test_bulk_insert_invariants(cfb, orc, kb, bits, bs, policy):
+    """Small config: 2^20 slots filled to 0.95 (996 147 keys, splitmix64 seed 1)."""
+    f, o = make(cfb, orc, kb, bits, bs, policy, 500, 1 << 20)
+    keys = orc.splitmix64(1, int(0.95 * f.capacity()))
+    if kb == 4:
+        keys = np.unique(keys.astype(np.uint32))
+    d = dev(keys)
+    ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
+    occ = f.insertMany(d, d_output=ok_t)
+    ok = host_u8(ok_t).astype(bool)
+    st = f.stats()
+    assert occ == ok.sum() == st["occupied"] == f.countOccupiedSlots()
+    assert st["lost"] == 0
+    assert st["primary"] + st["secondary"] + st["evicted_inserts"] == len(keys)
+    assert st["failed"] == len(keys) - ok.sum()
+    assert host_u8(f.containsMany(d[torch.from_numpy(ok).cuda()])).all(), "false negative"
+    errs = _stored_invariants(f, o, orc, keys[ok])
+    assert not errs, errs
+    # failure count within 3 sigma of the oracle's sequential fill of the same keys
+    n_ok_seq = o.insert(keys)
+    fail_gpu, fail_seq = len(keys) - int(ok.sum()), len(keys) - n_ok_seq
+    sigma = math.sqrt(max(fail_seq, 1) * (1 - fail_seq / len(keys)))
+    assert abs(fail_gpu - fail_seq) <= 3 * sigma + 3, (fail_gpu, fail_seq)
+
+
+@pytest.mark.parametrize("kb,bits,bs,policy", [(8, 16, 16, 0), (8, 8, 16, 1), (8, 32, 8, 0)])
+def test_false_positive_rate_within_3_sigma(cfb, orc, kb, bits, bs, policy):
+    f, o = make(cfb, orc, kb, bits, bs, policy, 500, 1 << 20)
+    keys = orc.splitmix64(1, int(0.95 * f.capacity()))
+    f.insertMany(dev(keys))
+    o.insert(keys)
+    neg = orc.splitmix64(2, 2_000_000)
+    neg = neg[~np.isin(neg, keys)]
+    fp_gpu = int(host_u8(f.containsMany(dev(neg))).sum())
+    fp_seq = int(o.contains(neg, threads=4).sum())
+    p = fp_seq / len(neg)
+    sigma = math.sqrt(len(neg) * p * (1 - p))
+    assert abs(fp_gpu - fp_seq) <= 3 * sigma + 3, (fp_gpu, fp_seq)
+    theory = 2 * bs * 0.95 / 2 ** bits
+    assert 0.5 * theory < fp_gpu / len(neg) < 1.5 * theory
+
+
+@pytest.mark.parametrize("kb,bits,bs", [(8, 16, 16), (8, 8, 16), (8, 32, 8), (4, 16, 16)])
+def test_sequential_delete_bit_exact(cfb, orc, kb, bits, bs):
+    f, o = make(cfb, orc, kb, bits, bs, 0, 500, 1 << 12)
+    keys = orc.splitmix64(55, int(0.9 * f.capacity()))
+    if kb == 4:
+        keys = keys.astype(np.uint32)
+    o.insert(keys)
+    f.load_table(torch.from_numpy(o.table).cuda())
+    dels = np.concatenate([keys[::3], orc.splitmix64(56, 200).astype(keys.dtype), keys[:50]])
+    d = dev(dels)
+    out = torch.empty(1, dtype=torch.bool, device="cuda")
+    got = np.empty(len(dels), np.uint8)
+    for i in range(len(dels)):
+        f.deleteMany(d[i:i + 1], out)
+        got[i] = int(out.item())
+    _, want = o.delete(dels)
+    assert np.array_equal(got, want)
+    assert np.array_equal(image(f), o.table)
+    assert f.occupiedSlots() == o.occupied()
+
+
+@pytest.mark.parametrize("kb,bits,bs,policy", [(8, 16, 16, 0), (8, 32, 8, 1), (4, 16, 16, 1)])
+def test_bulk_delete(cfb, orc, kb, bits, bs, policy):
+    """Insert at 0.95, delete the first half, re-query (the reference's example flow, src/main.cu:128-175)."""
+    f, o = make(cfb, orc, kb, bits, bs, policy, 500, 1 << 20)
+    keys = orc.splitmix64(1, int(0.95 * f.capacity()))
+    if kb == 4:
+        keys = np.unique(keys.astype(np.uint32))
+    d = dev(keys)
+    ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
+    occ0 = f.insertMany(d, d_output=ok_t)
+    ok = host_u8(ok_t).astype(bool)
+    stored = keys[ok]
+    half = len(stored) // 2
+    dd = dev(stored[:half])
+    out = torch.empty(half, dtype=torch.bool, device="cuda")
+    occ1 = f.deleteMany(dd, out)
+    assert host_u8(out).all(), "a stored key could not be deleted"
+    assert occ1 == occ0 - half == f.countOccupiedSlots()
+    assert host_u8(f.containsMany(dev(stored[half:]))).all(), "false negative after delete"
+    errs = _stored_invariants(f, o, orc, stored[half:])
+    assert not errs, errs
+
+
+def test_insert_delete_round_trip_empties_table(cfb, orc):
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 22)
+    keys = orc.splitmix64(7, int(0.95 * f.capacity()))
+    d = dev(keys)
+    ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
+    f.insertMany(d, d_output=ok_t)
+    stored = d[ok_t]
+    f.deleteMany(stored)
+    assert f.occupiedSlots() == 0
+    assert f.countOccupiedSlots() == 0
+
+
+def test_duplicate_keys_overflow_without_loss(cfb, orc):
+    """48 copies of one key: exactly 2*bs fit (both buckets), the rest fail and
+    undo their chains; nothing is lost."""
+    f, o = make(cfb, orc, 8, 16, 16, 1, 64, 1 << 12)
+    keys = np.full(48, 12345, dtype=np.uint64)
+    out = torch.empty(48, dtype=torch.bool, device="cuda")
+    occ = f.insertMany(dev(keys), d_output=out)
+    assert occ == 32 == int(host_u8(out).sum())
+    st = f.stats()
+    assert st["failed"] == 16 and st["lost"] == 0
+    assert f.countOccupiedSlots() == 32
+    n = f.deleteMany(dev(keys))
+    assert n == 0
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3, 5, 31, 33, 255, 257, 1023, 4097, 100_003])
+def test_ragged_sizes(cfb, orc, n):
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 18)
+    keys = orc.splitmix64(9, n)
+    d = dev(keys) if n else torch.empty(0, dtype=torch.int64, device="cuda")
+    out = torch.zeros(n, dtype=torch.bool, device="cuda")
+    assert f.insertMany(d, d_output=out) == n
+    assert host_u8(out).all()
+    res = f.containsMany(d)
+    assert host_u8(res).all()
+    assert f.deleteMany(d) == 0
+
+
+@pytest.mark.parametrize("offset", [1, 2, 3, 5])
+def test_unaligned_pointers(cfb, orc, offset):
+    """Key and output pointers that are not vector-aligned take the scalar path."""
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 16)
+    keys = orc.splitmix64(13, 40_000)
+    buf = dev(np.concatenate([np.zeros(offset, np.uint64), keys]))
+    d = buf[offset:]
+    assert d.data_ptr() % 32 != 0
+    outbuf = torch.zeros(len(keys) + offset, dtype=torch.bool, device="cuda")
+    out = outbuf[offset:]
+    f.insertMany(d, d_output=out)
+    assert host_u8(out).all()
+    o.insert(keys)
+    neg = orc.splitmix64(14, 30_000)
+    q = np.concatenate([keys, neg])
+    qb = dev(np.concatenate([np.zeros(offset, np.uint64), q]))
+    ob = torch.zeros(len(q) + offset, dtype=torch.bool, device="cuda")
+    f.containsMany(qb[offset:], ob[offset:])
+    got = host_u8(ob[offset:])
+    assert got[: len(keys)].all()
+    assert host_u8(ob[:offset]).sum() == 0, "wrote before the output start"
+    # lookups are a function of the table image alone
+    o2 = orc.OracleFilter(bits=16, bucket_size=16, capacity=1 << 16)
+    o2.table[:] = image(f)
+    assert np.array_equal(got, o2.contains(q, threads=4))
+
+
+def test_clear_and_counters(cfb, orc):
+    f, o = make(cfb, orc, 8, 16, 16, 1, 500, 10000)
+    keys = dev(np.array([1, 2, 3, 4, 5], dtype=np.uint64))
+    assert f.insertMany(keys) == 5
+    assert f.loadFactor() == pytest.approx(5 / f.capacity())
+    f.clear()
+    assert f.occupiedSlots() == 0 and f.countOccupiedSlots() == 0
+    assert not host_u8(f.containsMany(keys)).any()
+    assert f.stats()["primary"] == 0
