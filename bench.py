@@ -54,6 +54,11 @@ WORKLOADS = {
              "uint64 keys; fill 0.95 (splitmix64 seed 3); 2^28 lookups 50% positive; 2^26 deletes",
         capacity=1 << 31, bits=16, bs=16, policy="BFS", max_ev=500, fill=0.95,
         n_pos=1 << 27, n_neg=1 << 27, n_del=1 << 26, seed_fill=3, seed_neg=4, seed_sample=5),
+    "medium": dict(
+        desc="medium out-of-L2 filter for profiling: 2^28 slots, 16-bit tags, 16-slot buckets (512 MiB), BFS; "
+             "fill 0.95 (splitmix64 seed 3); 2^25 lookups 50% positive; 2^23 deletes",
+        capacity=1 << 28, bits=16, bs=16, policy="BFS", max_ev=500, fill=0.95,
+        n_pos=1 << 24, n_neg=1 << 24, n_del=1 << 23, seed_fill=3, seed_neg=4, seed_sample=5),
     "small": dict(
         desc="small filter (L2-resident): 2^20 slots, 16-bit tags, 16-slot buckets, BFS; 996147 keys "
              "(splitmix64 seed 1); lookups of all of them + 996147 negatives (seed 2); delete half",

@@ -215,17 +215,22 @@ __device__ __noinline__ bool evict_dfs(DevTable t, uint32_t fp, uint64_t start, 
 // insertWithEvictionBFS: up to min(8, bs/2) candidates of the start bucket are
 // moved to their alternate bucket (copy first, then swap fp in, undo the copy
 // if the candidate moved meanwhile); then DFS.
+//
+// The start bucket is read once (one vector load) and the candidates are taken
+// from that snapshot; the swap's compare-and-swap re-validates the candidate.
 template <class C>
-__device__ __noinline__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, uint64_t other, uint32_t max_ev,
-                                       EvictStats& st, bool& err) {
+__device__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, uint64_t other, uint32_t max_ev,
+                          EvictStats& st, bool& err) {
     constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
     constexpr uint32_t ncand = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
     uint64_t* sbw = bucket_words<C>(t, start);
+    uint64_t snap[C::nchunks];
+    load_rlx<C::bucket_bytes>(sbw, snap);
     for (uint32_t i = 0; i < ncand; ++i) {
         const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * i) & (C::bs - 1));
         const int w = static_cast<int>(slot / C::tpw);
         const int sh = static_cast<int>(slot % C::tpw) * C::bits;
-        uint64_t word = load_word_rlx(sbw + w);
+        uint64_t word = pick(snap, w);
         const uint32_t cand = static_cast<uint32_t>((word >> sh) & lane_mask);
         uint64_t c[C::nchunks];
         if (cand == 0) {
@@ -248,6 +253,7 @@ __device__ __noinline__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, 
             }
             load_rlx<C::bucket_bytes>(abw, c);
             try_remove<C>(abw, c, cand, err);
+            load_rlx<C::bucket_bytes>(sbw, snap);  // the start bucket changed under us
         }
         if (err) return false;
     }
@@ -407,70 +413,120 @@ __global__ void __launch_bounds__(512) k_delete(DevTable t, const typename C::Ke
     if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
 }
 
+// Eviction for one key whose two buckets were full (CuckooFilter::insert,
+// CuckooFilter.cuh:1066-1071): start at i1 if the tag is even, else at i2.
+template <class C>
+__device__ __noinline__ bool evict_key(DevTable t, uint64_t key, uint32_t policy_bfs, uint32_t max_ev,
+                                       EvictStats& st, bool& err) {
+    uint64_t i1;
+    uint32_t fp;
+    candidates<C>(key, t.nb_mask, i1, fp);
+    const uint64_t i2 = alt_bucket<C>(i1, fp, t.nb_mask);
+    const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
+    const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
+    return policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
+                      : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+}
+
+// Inclusive prefix sum across the warp.
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v) {
+    const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, v, d);
+        if (lane >= static_cast<uint32_t>(d)) v += u;
+    }
+    return v;
+}
+
+// insertMany.  Pass 1 per key: first empty slot of i1, else of i2.  Keys whose
+// two buckets are full are not evicted in place (one evicting lane would stall
+// its 31 neighbours for the whole chain); their indices are parked in a
+// per-warp shared-memory buffer and evicted 32 at a time, one key per lane.
 template <class C, int KPT>
 __global__ void __launch_bounds__(512) k_insert(DevTable t, const typename C::Key* __restrict__ keys, uint64_t n,
                                                 uint8_t* __restrict__ out, bool keys_vec, bool out_vec,
                                                 uint32_t policy_bfs, uint32_t max_ev) {
+    constexpr int kBuf = 32 + 32 * KPT;  // < 32 left over + one tile's worth
+    __shared__ uint64_t s_defer[16 * kBuf];
+    uint64_t* buf = s_defer + (threadIdx.x >> 5) * kBuf;
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t pending = 0;  // warp-uniform number of parked keys
     const uint64_t tile = static_cast<uint64_t>(blockDim.x) * KPT;
     uint32_t n_prim = 0, n_sec = 0, n_evk = 0, n_fail = 0;
     EvictStats st;
     bool err = false;
+
+    auto evict_parked = [&](uint64_t idx) {
+        const uint64_t key = C::key_bytes == 8 ? static_cast<uint64_t>(reinterpret_cast<const uint64_t*>(keys)[idx])
+                                               : static_cast<uint64_t>(reinterpret_cast<const uint32_t*>(keys)[idx]);
+        ++n_evk;
+        if (evict_key<C>(t, key, policy_bfs, max_ev, st, err)) {
+            if (out) out[idx] = 1;
+        } else {
+            ++n_fail;
+        }
+    };
+
     for (uint64_t base = blockIdx.x * tile; base < n; base += static_cast<uint64_t>(gridDim.x) * tile) {
         const uint64_t k0 = base + static_cast<uint64_t>(threadIdx.x) * KPT;
-        if (k0 >= n) continue;
+        uint32_t valid = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) valid |= (k0 + j < n ? 1u : 0u) << j;
         uint64_t key[KPT];
-        load_keys<C, KPT>(keys, k0, n, keys_vec, key);
         uint64_t b[KPT];
         uint32_t fp[KPT];
         uint64_t c[KPT][C::nchunks];
+        uint32_t done = 0;
+        if (valid) {
+            load_keys<C, KPT>(keys, k0, n, keys_vec, key);
 #pragma unroll
-        for (int j = 0; j < KPT; ++j) {
-            candidates<C>(key[j], t.nb_mask, b[j], fp[j]);
-            if (k0 + j < n) load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
-        }
-        uint32_t done = 0, valid = 0;
-#pragma unroll
-        for (int j = 0; j < KPT; ++j) {
-            if (k0 + j < n) {
-                valid |= 1u << j;
-                if (try_insert<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err)) done |= 1u << j;
+            for (int j = 0; j < KPT; ++j) {
+                candidates<C>(key[j], t.nb_mask, b[j], fp[j]);
+                if ((valid >> j) & 1u) load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
             }
-        }
-        n_prim += __popc(done);
-        uint64_t b2[KPT];
 #pragma unroll
-        for (int j = 0; j < KPT; ++j) {
-            b2[j] = 0;
-            if (((valid & ~done) >> j) & 1u) {
-                b2[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
-                load_rlx<C::bucket_bytes>(t.buckets + b2[j] * C::bucket_bytes, c[j]);
+            for (int j = 0; j < KPT; ++j)
+                if (((valid >> j) & 1u) && try_insert<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err)) done |= 1u << j;
+            n_prim += __popc(done);
+            const uint32_t miss = valid & ~done;
+            if (miss) {
+#pragma unroll
+                for (int j = 0; j < KPT; ++j) {
+                    if ((miss >> j) & 1u) {
+                        b[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
+                        load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
+                    }
+                }
+                uint32_t sec = 0;
+#pragma unroll
+                for (int j = 0; j < KPT; ++j)
+                    if (((miss >> j) & 1u) && try_insert<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err))
+                        sec |= 1u << j;
+                n_sec += __popc(sec);
+                done |= sec;
             }
+            if (out) store_results<KPT>(out, k0, n, out_vec, done);
         }
-        uint32_t sec = 0;
+        // park the keys whose buckets are both full
+        const uint32_t hard = valid & ~done;
+        const uint32_t cnt = __popc(hard);
+        const uint32_t incl = warp_inclusive_scan(cnt);
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint32_t pos = pending + incl - cnt;
 #pragma unroll
         for (int j = 0; j < KPT; ++j)
-            if (((valid & ~done) >> j) & 1u && try_insert<C>(bucket_words<C>(t, b2[j]), c[j], fp[j], err))
-                sec |= 1u << j;
-        n_sec += __popc(sec);
-        done |= sec;
-        const uint32_t hard = valid & ~done;
-        if (hard) {
-#pragma unroll 1
-            for (int j = 0; j < KPT; ++j) {
-                if (!((hard >> j) & 1u)) continue;
-                ++n_evk;
-                const uint64_t start = (fp[j] & 1u) == 0 ? b[j] : b2[j];
-                const uint64_t other = (fp[j] & 1u) == 0 ? b2[j] : b[j];
-                const bool ok = policy_bfs ? evict_bfs<C>(t, fp[j], start, other, max_ev, st, err)
-                                           : evict_dfs<C>(t, fp[j], start, other, max_ev, st, err);
-                if (ok)
-                    done |= 1u << j;
-                else
-                    ++n_fail;
-            }
+            if ((hard >> j) & 1u) buf[pos++] = k0 + j;
+        pending += total;
+        __syncwarp();  // parked indices and result bytes visible to the whole warp
+        while (pending >= 32) {
+            pending -= 32;
+            const uint64_t idx = buf[pending + lane];
+            __syncwarp();
+            evict_parked(idx);
         }
-        if (out) store_results<KPT>(out, k0, n, out_vec, done);
     }
+    if (lane < pending) evict_parked(buf[lane]);
     flush_counter(&t.ctr[CTR_OCCUPIED], n_prim + n_sec + (n_evk - n_fail));
     flush_counter(&t.ctr[CTR_PRIMARY], n_prim);
     flush_counter(&t.ctr[CTR_SECONDARY], n_sec);

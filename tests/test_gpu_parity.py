@@ -238,8 +238,11 @@ def test_false_positive_rate_within_3_sigma(cfb, orc, kb, bits, bs, policy):
     p = fp_seq / len(neg)
     sigma = math.sqrt(len(neg) * p * (1 - p))
     assert abs(fp_gpu - fp_seq) <= 3 * sigma + 3, (fp_gpu, fp_seq)
-    theory = 2 * bs * 0.95 / 2 ** bits
-    assert 0.5 * theory < fp_gpu / len(neg) < 1.5 * theory
+    theory = 2 * bs * 0.95 / 2 ** bits  # the reference's estimate, src/main.cu:114-115
+    if theory * len(neg) >= 100:
+        assert 0.5 * theory < fp_gpu / len(neg) < 1.5 * theory
+    else:
+        assert fp_gpu <= 3 + 3 * math.sqrt(theory * len(neg)) + theory * len(neg)
 
 
 @pytest.mark.parametrize("kb,bits,bs", [(8, 16, 16), (8, 8, 16), (8, 32, 8), (4, 16, 16)])
