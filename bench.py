@@ -353,10 +353,21 @@ def run_b200(args, w: dict) -> dict | None:
     cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=w["bits"], maxEvictions=w["max_ev"], blockSize=args.block,
                            bucketSize=w["bs"], evictionPolicy=cfb.EvictionPolicy[w["policy"]])
     f = cfb.CuckooFilter(cfg, w["capacity"])
+    f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
     fill, query, dele, n_coll = make_inputs(w, dev, rank)
     n_fill, n_q, n_d = fill.numel(), query.numel(), dele.numel()
     q_out = torch.empty(n_q, dtype=torch.bool, device=dev)
     torch.cuda.synchronize()
+    # the reference benchmark's adaptiveInsert (benchmark_common.cuh:113-126): sorted from 2^29 keys
+    sorted_fill = args.insert == "sorted" or (args.insert == "auto" and n_fill >= (1 << 29))
+
+    def fill_table(sync: bool):
+        if sorted_fill:
+            f.insertManySorted(fill, stream=stream)
+        elif sync:
+            f.insertMany(fill, stream=stream)
+        else:
+            f.insertManyAsync(fill, stream=stream)
 
     def step(ev=None):
         if ev:
@@ -364,10 +375,7 @@ def run_b200(args, w: dict) -> dict | None:
         f.clear(stream)  # synchronous memset of the table and counters
         if ev:
             ev[1].record(stream)
-        if args.sorted:
-            f.insertManySorted(fill, stream=stream)
-        else:
-            f.insertManyAsync(fill, stream=stream)
+        fill_table(False)
         if ev:
             ev[2].record(stream)
         f.containsManyAsync(query, q_out, stream=stream)
@@ -382,16 +390,14 @@ def run_b200(args, w: dict) -> dict | None:
     for i in range(args.warmup):
         f.clear(stream)
         f.resetEvictionCount()
-        if args.sorted:
-            f.insertManySorted(fill, stream=stream)
-        else:
-            f.insertMany(fill, stream=stream)
+        fill_table(True)
         st = f.stats()
         if i == 0:
             acct["i1_full"] = st["secondary"] + st["evicted_inserts"]
             acct["inserted"] = st["occupied"]
             acct["failed"] = st["failed"]
             acct["evictions"] = st["evictions"]
+            acct["fill_stats"] = st
             acct["q_primary"] = f.probe_count(query, stream=stream)
             acct["d_primary"] = f.probe_count(dele, stream=stream)
         f.containsManyAsync(query, q_out, stream=stream)
@@ -434,6 +440,29 @@ def run_b200(args, w: dict) -> dict | None:
     ops = {"insert": op(n_fill, ins_ms, ins_bytes), "contains": op(n_q, con_ms, con_bytes),
            "delete": op(n_d, del_ms, del_bytes), "clear_ms": statistics.mean(
                [evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)])}
+    ops["insert"]["path"] = "insertManySorted (segment-staged)" if sorted_fill else "insertMany (random CAS)"
+    # the library's automatic choice (CF_OPT_SEGMENTED_MIN_KEYS = 0): segment path from 8 keys per bucket
+    seg_q = n_q >= f.getNumBuckets() * 8
+    seg_d = n_d >= f.getNumBuckets() * 8
+    ops["contains"]["path"] = "segment-staged" if seg_q else "random probes"
+    ops["delete"]["path"] = "segment-staged" if seg_d else "random probes"
+
+    # plain insertMany (random CAS path) on the same fill, timed on its own
+    if sorted_fill and not args.no_plain:
+        ts = []
+        for _ in range(max(1, min(args.steps, 3))):
+            f.clear(stream)
+            f.resetEvictionCount()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            f.insertManyAsync(fill, stream=stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        st_p = f.stats()
+        ops["insert_plain"] = op(n_fill, ts, n_fill * 72 + 32 * (st_p["secondary"] + st_p["evicted_inserts"]))
+        ops["insert_plain"]["path"] = "insertMany (random CAS), not part of the step"
+        ops["insert_plain"]["failed"] = st_p["failed"]
     dom = max(("insert", "contains", "delete"), key=lambda k: ops[k]["ms"])
     traffic = load_traffic(dom, w)
     roof = {"bound": "hbm", "kernel": dom, "achieved": ops[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
@@ -498,7 +527,8 @@ def run_b200(args, w: dict) -> dict | None:
                        "num_buckets": f.getNumBuckets(), "table_bytes": f.sizeInBytes(),
                        "bits_per_tag": w["bits"], "bucket_size": w["bs"], "eviction": w["policy"],
                        "max_evictions": w["max_ev"], "block_size": args.block,
-                       "insert_path": "insertManySorted" if args.sorted else "insertMany",
+                       "insert_path": "insertManySorted" if sorted_fill else "insertMany",
+                       "workspace_limit_gb": args.workspace_gb,
                        "fill_keys": n_fill, "lookup_keys": n_q, "delete_keys": n_d,
                        "negatives_replaced": n_coll,
                        "l2": "inputs larger than L2 (table and key arrays exceed 126 MB); no flush needed"
@@ -595,7 +625,8 @@ def run_reference_gpu(args, w: dict) -> dict:
         ref.clear()
         e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         e[0].record(stream)
-        ref.insert(fill.data_ptr(), fill.numel(), stream.cuda_stream or None, bool(args.sorted))
+        ref.insert(fill.data_ptr(), fill.numel(), stream.cuda_stream or None,
+                   args.insert == "sorted" or (args.insert == "auto" and fill.numel() >= (1 << 29)))
         e[1].record(stream)
         ref.contains(query.data_ptr(), query.numel(), out.data_ptr(), stream.cuda_stream or None)
         e[2].record(stream)
@@ -627,7 +658,12 @@ def main() -> None:
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large")
     ap.add_argument("--block", type=int, default=256)
-    ap.add_argument("--sorted", action="store_true", help="use insertManySorted for the fill")
+    ap.add_argument("--insert", choices=("auto", "plain", "sorted"), default="auto",
+                    help="fill with insertMany (plain), insertManySorted (sorted), or as the reference's benchmark "
+                         "does (auto: sorted from 2^29 keys)")
+    ap.add_argument("--workspace-gb", type=float, default=40.0,
+                    help="workspace limit of the segment-staged path (CF_OPT_WORKSPACE_LIMIT)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the separate plain insertMany timing")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

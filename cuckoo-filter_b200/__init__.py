@@ -41,6 +41,14 @@ class CuckooError(RuntimeError):
         self.status = status
 
 
+# cf_option values (include/cuckoo_b200.h)
+OPT_WORKSPACE_LIMIT = 1
+OPT_SEGMENTED_MIN_KEYS = 2
+OPT_WORKSPACE_BYTES = 3
+OPT_ROUND2_SEGMENTED_MIN_KEYS = 4
+NEVER = (1 << 64) - 1
+
+
 class EvictionPolicy(enum.IntEnum):
     """Reference ``enum class EvictionPolicy`` (CuckooFilter.cuh:19-22)."""
 
@@ -61,7 +69,7 @@ class _Info(C.Structure):
 
 class _Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("occupied", "primary", "secondary", "evicted_inserts", "evictions",
-                                          "failed", "lost", "removed")]
+                                          "failed", "lost", "removed", "duplicates")]
 
 
 _lib: Optional[C.CDLL] = None
@@ -104,6 +112,8 @@ def library() -> C.CDLL:
         "cf_store_table": ([vp, vp, u64, vp], i32),
         "cf_probe_count": ([vp, vp, u64, P64, vp], i32),
         "cf_hash_candidates": ([C.POINTER(_Config), u64, vp, u64, vp, vp, vp], i32),
+        "cf_set_option": ([vp, i32, u64], i32),
+        "cf_get_option": ([vp, i32, P64], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -305,6 +315,15 @@ class CuckooFilter:
     def countOccupiedSlots(self) -> int:
         v = C.c_uint64()
         _check(library().cf_count_occupied_slots(self._h, C.byref(v)))
+        return int(v.value)
+
+    def setOption(self, option: int, value: int) -> None:
+        """cf_set_option: OPT_WORKSPACE_LIMIT (bytes) or OPT_SEGMENTED_MIN_KEYS (0 = automatic)."""
+        _check(library().cf_set_option(self._h, option, value))
+
+    def getOption(self, option: int) -> int:
+        v = C.c_uint64()
+        _check(library().cf_get_option(self._h, option, C.byref(v)))
         return int(v.value)
 
     def stats(self) -> dict:

@@ -31,6 +31,16 @@ struct cf_filter {
     int block;
     int max_grid[KID_COUNT_KERNELS];
     int max_grid_aux;
+    int sms;
+    // segment-staged path
+    bool seg_ok;            // packed (bucket, tag) entries fit in 64 bits
+    SegGeom geom;
+    void* ws;               // workspace (grown on demand, freed with the filter)
+    uint64_t ws_bytes;
+    uint64_t ws_limit;      // CF_OPT_WORKSPACE_LIMIT
+    uint64_t seg_min_keys;  // CF_OPT_SEGMENTED_MIN_KEYS (0 = automatic)
+    uint64_t round2_min;    // CF_OPT_ROUND2_SEGMENTED_MIN_KEYS (0 = automatic)
+    unsigned long long* h_cnt;
 };
 
 namespace {
@@ -157,6 +167,118 @@ int finish(cf_filter* f, void* stream, uint64_t* occupied_out) {
     return CF_OK;
 }
 
+int ilog2(uint64_t v) { return 63 - __builtin_clzll(v); }
+
+void init_geometry(cf_filter* f) {
+    const uint64_t bb = f->ops->bucket_bytes;
+    uint64_t sb = kSegBytes / bb;
+    if (sb > f->num_buckets) sb = f->num_buckets;
+    f->geom.sb_log2 = ilog2(sb);
+    f->geom.nseg = f->num_buckets / sb;
+    f->geom.seg_shift = static_cast<int>(f->cfg.bits_per_tag) + f->geom.sb_log2;
+    const int seg_bits = f->geom.nseg > 1 ? ilog2(f->geom.nseg) : 0;
+    f->geom.passes = seg_bits == 0 ? 1 : (seg_bits + kRadixBits - 1) / kRadixBits;
+    // (bucket << bits) | tag must fit in 64 bits for every bucket index
+    f->seg_ok = ilog2(f->num_buckets) + static_cast<int>(f->cfg.bits_per_tag) <= 64;
+}
+
+// Bytes of workspace for a chunk of `cap` keys: two entry buffers (8 B per
+// key), and with per-key results two payload buffers (4 B) and a result bitmap.
+uint64_t ws_need(const cf_filter* f, uint64_t cap, int grid, bool payload) {
+    const uint64_t hist = static_cast<uint64_t>(kRadix) * grid * 4;
+    const uint64_t start = (f->geom.nseg + 1) * 4;
+    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+    const uint64_t per_key = payload ? al(cap * 4) * 2 + al((cap + 31) / 32 * 4) : 0;
+    return al(cap * 8) * 2 + per_key + al(hist) + al(start) + al(64);
+}
+
+int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
+    // radix passes: one wave of the (heaviest) scatter kernel, fixed per-CTA chunks
+    static const int rs_bps = blocks_per_sm(k_rs_scatter<2>, kRsThreads, 0);
+    const int grid = f->sms * rs_bps;
+    const uint64_t fixed = ws_need(f, 0, grid, payload) + 4096;
+    uint64_t cap = n;
+    if (f->ws_limit > fixed) {
+        const uint64_t fit = (f->ws_limit - fixed) / (payload ? 25 : 16);
+        if (cap > fit) cap = fit;
+    } else {
+        cap = 0;
+    }
+    const uint64_t kMaxChunk = 1ull << 31;  // 32-bit positions and payloads
+    if (cap > kMaxChunk) cap = kMaxChunk;
+    if (cap < n) cap = cap / 32 * 32;
+    if (cap < 1024 && n > cap) cap = 1024;
+    const uint64_t need = ws_need(f, cap, grid, payload);
+    if (f->ws_bytes < need) {
+        if (f->ws) cudaFree(f->ws);
+        f->ws = nullptr;
+        f->ws_bytes = 0;
+        CF_CUDA(cudaMalloc(&f->ws, need), "workspace allocation");
+        f->ws_bytes = need;
+    }
+    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+    uint8_t* p = static_cast<uint8_t*>(f->ws);
+    w->ent[0] = reinterpret_cast<uint64_t*>(p);
+    p += al(cap * 8);
+    w->ent[1] = reinterpret_cast<uint64_t*>(p);
+    p += al(cap * 8);
+    w->hist = reinterpret_cast<uint32_t*>(p);
+    p += al(static_cast<uint64_t>(kRadix) * grid * 4);
+    w->start = reinterpret_cast<uint32_t*>(p);
+    p += al((f->geom.nseg + 1) * 4);
+    w->cnt = reinterpret_cast<unsigned long long*>(p);
+    p += al(64);
+    w->pay[0] = w->pay[1] = nullptr;
+    w->bitmap = nullptr;
+    if (payload) {
+        w->pay[0] = reinterpret_cast<uint32_t*>(p);
+        p += al(cap * 4);
+        w->pay[1] = reinterpret_cast<uint32_t*>(p);
+        p += al(cap * 4);
+        w->bitmap = reinterpret_cast<uint32_t*>(p);
+    }
+    w->h_cnt = f->h_cnt;
+    w->cap = cap;
+    w->grid = grid;
+    w->sms = f->sms;
+    return CF_OK;
+}
+
+// Keys from which the segment-staged path beats random probes: a random probe
+// costs one DRAM transaction, streaming a segment costs its bytes (read, and
+// write-back for insert/delete).
+// Measured on B200: a random probe costs one DRAM transaction (the device
+// completes ~38 G/s); the segment path costs its radix passes, the streamed
+// segments and the shared-memory work.  Lookups and deletes beat random
+// probing on the segment path only for batches of several keys per bucket;
+// the alternate-bucket round of a segment batch pays off from about one key
+// per 64 table bytes.
+uint64_t auto_threshold(const cf_filter* f, int op) {
+    if (op == SEG_INSERT) return f->table_bytes / 64;
+    return f->num_buckets * 8;
+}
+
+uint64_t segmented_threshold(const cf_filter* f, int op) {
+    return f->seg_min_keys ? f->seg_min_keys : auto_threshold(f, op);
+}
+
+int run_segmented(cf_filter* f, int op, const void* keys, uint64_t n, uint8_t* out, void* stream) {
+    if (n == 0) return CF_OK;
+    SegWork w{};
+    if (int st = ensure_workspace(f, n, out != nullptr, &w)) return st;
+    w.round2_segmented_min = f->round2_min ? f->round2_min : auto_threshold(f, op);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint64_t kb = f->cfg.key_bytes;
+    for (uint64_t c0 = 0; c0 < n; c0 += w.cap) {
+        const uint64_t m = n - c0 < w.cap ? n - c0 : w.cap;
+        CF_CUDA(f->ops->seg_chunk(dev(f), f->geom, w, op, static_cast<const uint8_t*>(keys) + c0 * kb, m,
+                                  out ? out + c0 : nullptr, s, f->cfg.eviction_policy == CF_EVICT_BFS ? 1u : 0u,
+                                  f->cfg.max_evictions),
+                "segment-staged batch");
+    }
+    return CF_OK;
+}
+
 int do_insert(cf_filter* f, const void* keys, uint64_t n, uint8_t* out, void* stream) {
     CF_CUDA(f->ops->insert(dev(f), keys, n, out, launch(f, KID_INSERT, stream),
                            f->cfg.eviction_policy == CF_EVICT_BFS ? 1u : 0u, f->cfg.max_evictions),
@@ -244,6 +366,10 @@ int cf_create(const cf_config* cfg, uint64_t capacity, cf_filter** out) {
         f->max_grid[k] = sms * (bps > 0 ? bps : 1);
     }
     f->max_grid_aux = sms * 8;
+    f->sms = sms;
+    init_geometry(f);
+    f->ws_limit = 4ull << 30;
+    if (e == cudaSuccess) e = cudaHostAlloc(&f->h_cnt, 4 * sizeof(unsigned long long), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMalloc(&f->d_table, f->table_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&f->d_ctr, CTR_COUNT * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaHostAlloc(&f->h_ctr, CTR_COUNT * sizeof(unsigned long long), cudaHostAllocDefault);
@@ -265,6 +391,8 @@ int cf_destroy(cf_filter* f) {
     if (f->d_table) cudaFree(f->d_table);
     if (f->d_ctr) cudaFree(f->d_ctr);
     if (f->h_ctr) cudaFreeHost(f->h_ctr);
+    if (f->h_cnt) cudaFreeHost(f->h_cnt);
+    if (f->ws) cudaFree(f->ws);
     delete f;
     return CF_OK;
 }
@@ -296,16 +424,21 @@ int cf_insert(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void
 int cf_insert_sorted(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,
                      uint64_t* occupied_out) {
     if (int s = check_batch(f, d_keys, n)) return s;
-    (void)d_out;
-    (void)stream;
-    (void)occupied_out;
-    return fail(CF_ERR_UNSUPPORTED, "insertManySorted is not built yet");
+    DeviceGuard g(f->device);
+    if (f->seg_ok) {
+        if (int s = run_segmented(f, SEG_INSERT, d_keys, n, d_out, stream)) return s;
+    } else {
+        // (bucket << bits) | tag does not fit 64 bits: the plain path
+        if (int s = do_insert(f, d_keys, n, d_out, stream)) return s;
+    }
+    return finish(f, stream, occupied_out);
 }
 
 int cf_contains_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
     if (int s = check_batch(f, d_keys, n)) return s;
     if (n && !d_out) return fail(CF_ERR_INVALID, "d_out is NULL with n > 0");
     DeviceGuard g(f->device);
+    if (f->seg_ok && n >= segmented_threshold(f, SEG_CONTAINS)) return run_segmented(f, SEG_CONTAINS, d_keys, n, d_out, stream);
     CF_CUDA(f->ops->contains(dev(f), d_keys, n, d_out, launch(f, KID_CONTAINS, stream)), "contains launch");
     return CF_OK;
 }
@@ -320,6 +453,7 @@ int cf_contains(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, vo
 int cf_delete_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
     if (int s = check_batch(f, d_keys, n)) return s;
     DeviceGuard g(f->device);
+    if (f->seg_ok && n >= segmented_threshold(f, SEG_DELETE)) return run_segmented(f, SEG_DELETE, d_keys, n, d_out, stream);
     CF_CUDA(f->ops->remove(dev(f), d_keys, n, d_out, launch(f, KID_DELETE, stream)), "delete launch");
     return CF_OK;
 }
@@ -380,6 +514,7 @@ int cf_get_stats(cf_filter* f, cf_stats* out) {
     out->failed = c[CTR_FAILED];
     out->lost = c[CTR_LOST];
     out->removed = c[CTR_REMOVED];
+    out->duplicates = c[CTR_DUP];
     return CF_OK;
 }
 
@@ -410,6 +545,35 @@ int cf_load_table(cf_filter* f, const void* src, uint64_t bytes, void* stream) {
     CF_CUDA(f->ops->count(dev(f), f->num_buckets, f->d_ctr + CTR_OCCUPIED, launch_aux(f, stream)), "recount");
     CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
     return CF_OK;
+}
+
+int cf_set_option(cf_filter* f, int option, uint64_t value) {
+    if (int s = check_filter(f)) return s;
+    switch (option) {
+        case CF_OPT_WORKSPACE_LIMIT:
+            f->ws_limit = value;
+            return CF_OK;
+        case CF_OPT_SEGMENTED_MIN_KEYS:
+            f->seg_min_keys = value;
+            return CF_OK;
+        case CF_OPT_ROUND2_SEGMENTED_MIN_KEYS:
+            f->round2_min = value;
+            return CF_OK;
+        default:
+            return fail(CF_ERR_INVALID, "unknown option %d", option);
+    }
+}
+
+int cf_get_option(cf_filter* f, int option, uint64_t* value) {
+    if (int s = check_filter(f)) return s;
+    if (!value) return fail(CF_ERR_INVALID, "value is NULL");
+    switch (option) {
+        case CF_OPT_WORKSPACE_LIMIT: *value = f->ws_limit; return CF_OK;
+        case CF_OPT_SEGMENTED_MIN_KEYS: *value = f->seg_min_keys; return CF_OK;
+        case CF_OPT_WORKSPACE_BYTES: *value = f->ws_bytes; return CF_OK;
+        case CF_OPT_ROUND2_SEGMENTED_MIN_KEYS: *value = f->round2_min; return CF_OK;
+        default: return fail(CF_ERR_INVALID, "unknown option %d", option);
+    }
 }
 
 int cf_store_table(cf_filter* f, void* dst, uint64_t bytes, void* stream) {

@@ -166,17 +166,19 @@ __device__ __forceinline__ int lowest_lane(uint64_t mask) {
 // ------------------------------------------------------------------- loads
 
 // Read-only bucket load through the non-coherent path, no L1 allocation (the
-// table is not written while a lookup batch runs).
+// table is not written while a lookup batch runs).  The non-coherent loads
+// here are not `volatile`: their data does not change during a kernel, so the
+// compiler may batch and hoist them.
 template <int BYTES>
 __device__ __forceinline__ void load_nc(const void* p, uint64_t* c) {
     if constexpr (BYTES == 8) {
-        asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(c[0]) : "l"(p));
+        asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(c[0]) : "l"(p));
     } else if constexpr (BYTES == 16) {
-        asm volatile("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];" : "=l"(c[0]), "=l"(c[1]) : "l"(p));
+        asm("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];" : "=l"(c[0]), "=l"(c[1]) : "l"(p));
     } else {
 #pragma unroll
         for (int i = 0; i < BYTES / 32; ++i) {
-            asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+            asm("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
                          : "=l"(c[4 * i]), "=l"(c[4 * i + 1]), "=l"(c[4 * i + 2]), "=l"(c[4 * i + 3])
                          : "l"(static_cast<const char*>(p) + 32 * i));
         }
@@ -218,23 +220,23 @@ __device__ __forceinline__ uint64_t cas64(uint64_t* p, uint64_t expected, uint64
 // Streaming key loads (read once).
 __device__ __forceinline__ uint64_t ld_stream_u64(const uint64_t* p) {
     uint64_t v;
-    asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
     return v;
 }
 __device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p) {
     uint32_t v;
-    asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
 }
 __device__ __forceinline__ void ld_stream_v4u64(const uint64_t* p, uint64_t& a, uint64_t& b, uint64_t& c,
                                                 uint64_t& d) {
-    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+    asm("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
                  : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
                  : "l"(p));
 }
 __device__ __forceinline__ void ld_stream_v4u32(const uint32_t* p, uint32_t& a, uint32_t& b, uint32_t& c,
                                                 uint32_t& d) {
-    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
                  : "l"(p));
 }

@@ -47,6 +47,7 @@ enum Counter : int {
     CTR_LOST = 6,
     CTR_ERROR = 7,
     CTR_REMOVED = 8,
+    CTR_DUP = 9,
     CTR_COUNT = 16
 };
 constexpr uint64_t ERR_CAS_LIMIT = 1;
@@ -162,8 +163,30 @@ __device__ uint32_t exchange_slot(uint64_t* bw, uint32_t slot, uint32_t v, bool&
 
 struct EvictStats {
     uint32_t evictions = 0;
-    uint32_t lost = 0;
+    uint32_t lost = 0;  // stored tags dropped when eviction walks crossed
+    uint32_t dup = 0;   // BFS copies that could not be taken back (an extra entry)
 };
+
+// Undo of a BFS copy (reference CuckooFilter.cuh:1011-1012): remove one instance
+// of `tag` from its bucket pair {a, b}.  While the copy was in place another
+// walk may have moved it to the other bucket of the pair, or be carrying an
+// instance between the two, so both buckets are tried, a bounded number of
+// times.  Any instance will do: equal tags of one pair are interchangeable.
+template <class C>
+__device__ bool remove_from_pair(const DevTable& t, uint64_t a, uint64_t b, uint32_t tag, bool& err) {
+    for (int it = 0; it < 1024; ++it) {
+        uint64_t c[C::nchunks];
+        uint64_t* aw = bucket_words<C>(t, a);
+        load_rlx<C::bucket_bytes>(aw, c);
+        if (try_remove<C>(aw, c, tag, err)) return true;
+        uint64_t* bw = bucket_words<C>(t, b);
+        load_rlx<C::bucket_bytes>(bw, c);
+        if (try_remove<C>(bw, c, tag, err)) return true;
+        if (err) return false;
+        __nanosleep(100);
+    }
+    return false;
+}
 
 // insertWithEvictionDFS with undo.  Returns true when fp is stored.
 template <class C>
@@ -251,8 +274,7 @@ __device__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, uint64_t othe
                     return true;
                 }
             }
-            load_rlx<C::bucket_bytes>(abw, c);
-            try_remove<C>(abw, c, cand, err);
+            if (!remove_from_pair<C>(t, ab, start, cand, err)) ++st.dup;
             load_rlx<C::bucket_bytes>(sbw, snap);  // the start bucket changed under us
         }
         if (err) return false;
@@ -527,7 +549,9 @@ __global__ void __launch_bounds__(512) k_insert(DevTable t, const typename C::Ke
         }
     }
     if (lane < pending) evict_parked(buf[lane]);
-    flush_counter(&t.ctr[CTR_OCCUPIED], n_prim + n_sec + (n_evk - n_fail));
+    // a tag dropped by crossing eviction walks leaves the table one entry short
+    flush_counter(&t.ctr[CTR_OCCUPIED], n_prim + n_sec + (n_evk - n_fail) - st.lost + st.dup);
+    flush_counter(&t.ctr[CTR_DUP], st.dup);
     flush_counter(&t.ctr[CTR_PRIMARY], n_prim);
     flush_counter(&t.ctr[CTR_SECONDARY], n_sec);
     flush_counter(&t.ctr[CTR_EVICTED_INSERTS], n_evk);

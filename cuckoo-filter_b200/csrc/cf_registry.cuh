@@ -12,8 +12,32 @@
 #include <vector>
 
 #include "cf_kernels.cuh"
+#include "cf_segmented.cuh"
 
 namespace cfb {
+
+// Geometry of the segment-staged path for one filter.
+struct SegGeom {
+    int sb_log2;     // log2 buckets per segment
+    int seg_shift;   // packed entry >> seg_shift = segment id
+    int passes;      // radix passes (8-bit digits) over the segment id
+    uint64_t nseg;   // segments
+};
+
+// Device workspace of the segment-staged path for a chunk of `cap` keys.
+struct SegWork {
+    uint64_t* ent[2];
+    uint32_t* pay[2];
+    uint32_t* hist;   // kRadix * grid
+    uint32_t* start;  // nseg + 1
+    unsigned long long* cnt;   // [2] list lengths
+    unsigned long long* h_cnt; // pinned mirror
+    uint32_t* bitmap;          // cap / 32 words
+    uint64_t cap;
+    int grid;      // radix CTAs (one wave of the scatter kernel)
+    int sms;       // streaming multiprocessors
+    uint64_t round2_segmented_min;  // list length from which round 2 is segment-staged
+};
 
 // Keys per thread of each batch kernel.
 constexpr int kContainsKPT = 4;
@@ -39,9 +63,19 @@ struct OpsTable {
     cudaError_t (*count)(const DevTable&, uint64_t nb, unsigned long long* result, const LaunchCfg&);
     cudaError_t (*probe)(const DevTable&, const void*, uint64_t, unsigned long long*, const LaunchCfg&);
     cudaError_t (*occupancy)(int kid, int block, int* blocks_per_sm);
+    cudaError_t (*seg_chunk)(const DevTable&, const SegGeom&, const SegWork&, int op, const void* keys, uint64_t m,
+                             uint8_t* out, cudaStream_t, uint32_t policy_bfs, uint32_t max_ev);
 };
 
 inline bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+// Blocks of `kernel` resident on one SM (at least 1).
+template <class K>
+int blocks_per_sm(K kernel, int threads, size_t smem) {
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, smem) != cudaSuccess || bps < 1) bps = 1;
+    return bps;
+}
 
 inline int grid_for(uint64_t n, int block, int kpt, int max_grid) {
     const uint64_t tile = static_cast<uint64_t>(block) * kpt;
@@ -107,6 +141,139 @@ struct Launchers {
         }
     }
 
+    // One radix pass: items [0, n) of `src` (keys when keys_mode) scattered by
+    // digit `shift` into dst.
+    // One radix pass over n items.  keys_mode: `src` is the key array; the
+    // histogram kernel hashes each key once and writes its packed entry to
+    // ent[1], which the scatter then reads (payload = the key's position).
+    // Otherwise `src` is ent[from] with payloads pay[from].  Scatters to ent[dst].
+    static cudaError_t rs_pass(bool keys_mode, bool payload, const DevTable& t, const void* src, int from, uint64_t n,
+                               int shift, int dst, const SegWork& w, cudaStream_t s) {
+        const uint32_t hist_n = static_cast<uint32_t>(kRadix) * static_cast<uint32_t>(w.grid);
+        const uint64_t* ent_src;
+        if (keys_mode) {
+            k_rs_hist<C, true><<<w.grid, kRsThreads, 0, s>>>(src, t.nb_mask, n, nullptr, shift, w.hist, w.ent[1]);
+            ent_src = w.ent[1];
+        } else {
+            ent_src = w.ent[from];
+            k_rs_hist<C, false><<<w.grid, kRsThreads, 0, s>>>(ent_src, t.nb_mask, n, nullptr, shift, w.hist, nullptr);
+        }
+        k_scan_u32<<<1, 1024, 0, s>>>(w.hist, hist_n);
+        if (!payload)
+            k_rs_scatter<0><<<w.grid, kRsThreads, 0, s>>>(ent_src, nullptr, n, nullptr, shift, w.hist, w.ent[dst],
+                                                          nullptr);
+        else if (keys_mode)
+            k_rs_scatter<1><<<w.grid, kRsThreads, 0, s>>>(ent_src, nullptr, n, nullptr, shift, w.hist, w.ent[dst],
+                                                          w.pay[dst]);
+        else
+            k_rs_scatter<2><<<w.grid, kRsThreads, 0, s>>>(ent_src, w.pay[from], n, nullptr, shift, w.hist,
+                                                          w.ent[dst], w.pay[dst]);
+        return cudaGetLastError();
+    }
+
+    // Sort n items by segment id; returns the index of the buffer holding the
+    // result.  keys_mode: the source is the key array; otherwise ent/pay[from].
+    static cudaError_t sort_by_segment(bool keys_mode, bool payload, const DevTable& t, const SegGeom& g,
+                                       const SegWork& w, const void* keys, int from, uint64_t n, cudaStream_t s,
+                                       int* result) {
+        int cur = from;
+        for (int p = 0; p < g.passes; ++p) {
+            const bool from_keys = keys_mode && p == 0;
+            const int dst = from_keys ? 0 : 1 - cur;
+            cudaError_t e = rs_pass(from_keys, payload, t, from_keys ? keys : nullptr, cur, n,
+                                    g.seg_shift + kRadixBits * p, dst, w, s);
+            if (e != cudaSuccess) return e;
+            cur = dst;
+        }
+        *result = cur;
+        return cudaSuccess;
+    }
+
+    template <int OP>
+    static cudaError_t seg_round(const DevTable& t, const SegGeom& g, const SegWork& w, int buf, bool payload,
+                                 int round, uint64_t n, cudaStream_t s) {
+        static bool attr_set = false;
+        const int smem = static_cast<int>((1ull << g.sb_log2) * C::bucket_bytes);
+        if (!attr_set) {
+            cudaError_t e = cudaFuncSetAttribute(k_seg<C, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSegBytes);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+        const uint64_t bthreads = n / 8 + 1;  // 8 positions per thread
+        const int bgrid = static_cast<int>((bthreads + 255) / 256 < 4096 ? (bthreads + 255) / 256 : 4096);
+        k_seg_bounds<<<bgrid, 256, 0, s>>>(w.ent[buf], n, nullptr, g.seg_shift, g.nseg, w.start);
+        const int other = 1 - buf;
+        // one wave: every resident CTA gets an equal share of the segments
+        static const int bps = blocks_per_sm(k_seg<C, OP>, kSegThreads, kSegBytes);
+        k_seg<C, OP><<<w.sms * bps, kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start,
+                                                           g.nseg, g.sb_log2, round, w.ent[other],
+                                                           payload ? w.pay[other] : nullptr, &w.cnt[round - 1],
+                                                           payload ? w.bitmap : nullptr);
+        return cudaGetLastError();
+    }
+
+    template <int OP>
+    static cudaError_t seg_chunk_op(const DevTable& t, const SegGeom& g, const SegWork& w, const void* keys,
+                                    uint64_t m, uint8_t* out, cudaStream_t s, uint32_t policy_bfs, uint32_t max_ev) {
+        const bool payload = out != nullptr;
+        cudaError_t e = cudaMemsetAsync(w.cnt, 0, 4 * sizeof(unsigned long long), s);
+        if (e == cudaSuccess && payload) e = cudaMemsetAsync(w.bitmap, 0, (m + 31) / 32 * 4, s);
+        int a = 0;
+        if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a);
+        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, s);
+        // round 2: keys that missed their primary bucket, now in ent/pay[1 - a]
+        if (e == cudaSuccess) e = cudaMemcpyAsync(w.h_cnt, w.cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return e;
+        const uint64_t m2 = w.h_cnt[0];
+        const int b = 1 - a;
+        if (m2 > 0) {
+            if (m2 >= w.round2_segmented_min) {
+                int c = b;
+                e = sort_by_segment(false, payload, t, g, w, nullptr, b, m2, s, &c);
+                if (e == cudaSuccess) e = seg_round<OP>(t, g, w, c, payload, 2, m2, s);
+                if (e == cudaSuccess && OP == SEG_INSERT) {
+                    // keys whose two buckets are full: ent/pay[1 - c], count cnt[1]
+                    uint32_t* bm = payload ? w.bitmap : nullptr;
+                    static const int bfs_bps = blocks_per_sm(k_evict_bfs_steps<C>, 256, 0);
+                    static const int list_bps = blocks_per_sm(k_evict_list<C>, 256, 0);
+                    if (policy_bfs) {
+                        k_evict_bfs_steps<C><<<w.sms * bfs_bps, 256, 0, s>>>(t, w.ent[1 - c],
+                                                                           payload ? w.pay[1 - c] : nullptr,
+                                                                           &w.cnt[1], bm, w.ent[c],
+                                                                           payload ? w.pay[c] : nullptr, &w.cnt[2]);
+                        k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[c], payload ? w.pay[c] : nullptr,
+                                                                        &w.cnt[2], 0u, max_ev, bm, 1u);
+                    } else {
+                        k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[1 - c],
+                                                                        payload ? w.pay[1 - c] : nullptr, &w.cnt[1],
+                                                                        0u, max_ev, bm, 0u);
+                    }
+                }
+            } else {
+                const int lgrid = static_cast<int>((m2 + 255) / 256 < 8192 ? (m2 + 255) / 256 : 8192);
+                k_list_random<C, OP><<<lgrid, 256, 0, s>>>(t, w.ent[b], payload ? w.pay[b] : nullptr, &w.cnt[0],
+                                                          policy_bfs, max_ev, payload ? w.bitmap : nullptr);
+            }
+            if (e == cudaSuccess) e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && payload) {
+            const int xgrid = static_cast<int>(((m + 31) / 32 + 255) / 256 < 8192 ? ((m + 31) / 32 + 255) / 256 : 8192);
+            k_bitmap_expand<<<xgrid, 256, 0, s>>>(w.bitmap, m, out);
+            e = cudaGetLastError();
+        }
+        return e;
+    }
+
+    static cudaError_t seg_chunk(const DevTable& t, const SegGeom& g, const SegWork& w, int op, const void* keys,
+                                 uint64_t m, uint8_t* out, cudaStream_t s, uint32_t policy_bfs, uint32_t max_ev) {
+        switch (op) {
+            case SEG_INSERT: return seg_chunk_op<SEG_INSERT>(t, g, w, keys, m, out, s, policy_bfs, max_ev);
+            case SEG_CONTAINS: return seg_chunk_op<SEG_CONTAINS>(t, g, w, keys, m, out, s, policy_bfs, max_ev);
+            default: return seg_chunk_op<SEG_DELETE>(t, g, w, keys, m, out, s, policy_bfs, max_ev);
+        }
+    }
+
     static OpsTable table() {
         OpsTable o{};
         o.key_bytes = C::key_bytes;
@@ -123,6 +290,7 @@ struct Launchers {
         o.count = count;
         o.probe = probe;
         o.occupancy = occupancy;
+        o.seg_chunk = seg_chunk;
         return o;
     }
 };

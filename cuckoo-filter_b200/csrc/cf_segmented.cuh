@@ -1,0 +1,766 @@
+// cf_segmented.cuh -- segment-staged batch execution.
+//
+// Random 32-byte probes of an out-of-L2 table are capped by the number of DRAM
+// transactions the memory system completes per second, not by bandwidth: on
+// B200 each random probe costs one transaction (128 B fetched) and the device
+// completes about 38 G of them per second, whatever the load width or path.
+// For batches that are large relative to the table this path instead
+//   1. radix-partitions the batch by table segment (packed (bucket << bits) |
+//      tag entries, 8-bit digits, stable, shared-memory staging so every write
+//      is a coalesced run),
+//   2. streams each 64 KiB table segment once into shared memory, applies all of
+//      the segment's operations there with shared-memory compare-and-swap, and
+//      writes the segment back with coalesced stores,
+//   3. repeats 1-2 for the keys that missed their primary bucket, keyed by the
+//      alternate bucket,
+//   4. (insert) evicts for the remaining keys with the random-access BFS/DFS.
+// This is the reference's insertManySorted idea (sort by primary bucket so the
+// writes coalesce, CuckooFilter.cuh:475-508 and :1209-1266) carried to its end:
+// the sort is only as fine as a shared-memory segment, and lookups and deletes
+// use it too.
+//
+// Per-key semantics are the plain path's: a key's tag goes to the first empty
+// slot of its primary bucket, else of its alternate, else eviction starts at
+// i1 for an even tag and i2 for an odd one.  One key alone takes exactly the
+// plain path's steps.
+#pragma once
+
+#include <cstdint>
+
+#include "cf_kernels.cuh"
+
+namespace cfb {
+
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kRsThreads = 256;
+constexpr int kRsWarps = kRsThreads / 32;
+constexpr int kRsIPT = 8;
+constexpr int kRsTile = kRsThreads * kRsIPT;
+constexpr int kSegBytes = 65536;
+constexpr int kSegThreads = 256;
+
+template <class C>
+__device__ __forceinline__ uint64_t pack_entry(uint64_t bucket, uint32_t fp) {
+    return (bucket << C::bits) | fp;
+}
+
+template <class C>
+__device__ __forceinline__ uint64_t key_entry(const void* keys, uint64_t i, uint64_t nb_mask) {
+    uint64_t key;
+    if constexpr (C::key_bytes == 8)
+        key = ld_stream_u64(static_cast<const uint64_t*>(keys) + i);
+    else
+        key = ld_stream_u32(static_cast<const uint32_t*>(keys) + i);
+    uint64_t b;
+    uint32_t fp;
+    candidates<C>(key, nb_mask, b, fp);
+    return pack_entry<C>(b, fp);
+}
+
+// Number of items of a radix pass: fixed, or read from a device counter.
+__device__ __forceinline__ uint64_t item_count(uint64_t n, const unsigned long long* n_dev) {
+    return n_dev ? static_cast<uint64_t>(*n_dev) : n;
+}
+
+__device__ __forceinline__ uint64_t chunk_of(uint64_t n) {
+    const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
+    return (per + kRsTile - 1) / kRsTile * kRsTile;
+}
+
+// Per-CTA digit histogram of its contiguous chunk: hist[digit * grid + cta].
+// KEYS: items are keys, hashed here into packed entries that are also written
+// to `ent_out` (so later passes never hash again); otherwise packed entries.
+template <class C, bool KEYS>
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const void* src, uint64_t nb_mask, uint64_t n,
+                                                        const unsigned long long* n_dev, int shift, uint32_t* hist,
+                                                        uint64_t* ent_out) {
+    __shared__ uint32_t cnt[kRadix];
+    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    const uint64_t m = item_count(n, n_dev);
+    const uint64_t chunk = chunk_of(m);
+    const uint64_t lo = blockIdx.x * chunk;
+    const uint64_t hi = lo + chunk < m ? lo + chunk : m;
+    constexpr int U = 8;  // independent loads in flight per thread
+    for (uint64_t b = lo; b < hi; b += static_cast<uint64_t>(blockDim.x) * U) {
+        uint64_t e[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint64_t i = b + static_cast<uint64_t>(j) * blockDim.x + threadIdx.x;
+            e[j] = 0;
+            if (i < hi) e[j] = KEYS ? key_entry<C>(src, i, nb_mask) : static_cast<const uint64_t*>(src)[i];
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint64_t i = b + static_cast<uint64_t>(j) * blockDim.x + threadIdx.x;
+            if (i < hi) {
+                atomicAdd(&cnt[(e[j] >> shift) & (kRadix - 1)], 1u);
+                if constexpr (KEYS) ent_out[i] = e[j];
+            }
+        }
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x] = cnt[d];
+}
+
+// Exclusive scan of `count` uint32 values in place (one CTA of 1024 threads).
+static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t count) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < count; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t x = i < count ? v[i] : 0u;
+        const uint32_t incl = warp_inclusive_scan(x);
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t t = warp_tot[lane];
+            warp_tot[lane] = warp_inclusive_scan(t) - t;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + warp_tot[warp] + incl - x;
+        if (i < count) v[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + x;
+        __syncthreads();
+    }
+}
+
+// One stable LSD pass over packed entries: scatter them to dst by digit, using
+// the scanned histogram as the CTA's starting offset per digit.  Each
+// 2048-entry tile is ranked in shared memory (lanes with equal digits found by
+// eight ballots, then warp order, then tile order), staged in digit order, and
+// written out as contiguous runs.  PAY: 0 = no payload, 1 = the payload of
+// entry i is i itself, 2 = payloads read from src_pay.
+template <int PAY>
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __restrict__ src,
+                                                           const uint32_t* __restrict__ src_pay, uint64_t n,
+                                                           const unsigned long long* n_dev, int shift,
+                                                           const uint32_t* offs, uint64_t* __restrict__ dst,
+                                                           uint32_t* __restrict__ dst_pay) {
+    __shared__ uint32_t running[kRadix];
+    __shared__ uint32_t tot[kRadix];
+    __shared__ uint32_t tile_off[kRadix];
+    __shared__ uint32_t warp_cnt[kRsWarps][kRadix];
+    __shared__ uint32_t scan_tmp[kRsWarps];
+    __shared__ uint64_t stage[kRsTile];
+    __shared__ uint32_t stage_pay[PAY ? kRsTile : 1];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint64_t m = item_count(n, n_dev);
+    const uint64_t chunk = chunk_of(m);
+    const uint64_t lo = blockIdx.x * chunk;
+    const uint64_t hi = lo + chunk < m ? lo + chunk : m;
+    for (int d = tid; d < kRadix; d += blockDim.x) running[d] = offs[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x];
+    for (uint64_t tb = lo; tb < hi; tb += kRsTile) {
+        for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&warp_cnt[0][0])[i] = 0;
+        __syncthreads();
+        uint64_t e[kRsIPT];
+        uint32_t p[kRsIPT];
+        uint32_t rank[kRsIPT];
+        uint32_t dig[kRsIPT];
+        // all loads of the tile first, so they are in flight together
+#pragma unroll
+        for (int j = 0; j < kRsIPT; ++j) {
+            const uint64_t i = tb + warp * 32 * kRsIPT + j * 32 + lane;
+            e[j] = 0;
+            p[j] = 0;
+            if (i < hi) {
+                e[j] = __ldcs(reinterpret_cast<const unsigned long long*>(src) + i);
+                if constexpr (PAY == 1) p[j] = static_cast<uint32_t>(i);
+                if constexpr (PAY == 2) p[j] = __ldcs(reinterpret_cast<const unsigned int*>(src_pay) + i);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kRsIPT; ++j) {
+            const uint64_t i = tb + warp * 32 * kRsIPT + j * 32 + lane;
+            const bool v = i < hi;
+            const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
+            dig[j] = v ? d : kRadix;
+            // lanes holding a valid entry with the same digit
+            uint32_t peers = __ballot_sync(0xFFFFFFFFu, v);
+#pragma unroll
+            for (int b = 0; b < kRadixBits; ++b) {
+                const uint32_t bit = (d >> b) & 1u;
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+                peers &= bit ? bal : ~bal;
+            }
+            const int leader = v ? __ffs(peers) - 1 : static_cast<int>(lane);
+            uint32_t base = 0;
+            if (v && static_cast<int>(lane) == leader) {
+                base = warp_cnt[warp][d];
+                warp_cnt[warp][d] = base + __popc(peers);
+            }
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            rank[j] = base + __popc(peers & lt_mask);
+            __syncwarp();
+        }
+        __syncthreads();
+        // per digit: exclusive prefix over warps, and the tile total
+        if (tid < kRadix) {
+            uint32_t s = 0;
+#pragma unroll
+            for (int w = 0; w < kRsWarps; ++w) {
+                const uint32_t c = warp_cnt[w][tid];
+                warp_cnt[w][tid] = s;
+                s += c;
+            }
+            tot[tid] = s;
+        }
+        __syncthreads();
+        // exclusive scan of the tile totals over digits (kRadix == kRsThreads)
+        {
+            const uint32_t x = tot[tid];
+            const uint32_t incl = warp_inclusive_scan(x);
+            if (lane == 31) scan_tmp[warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                const uint32_t t = lane < kRsWarps ? scan_tmp[lane] : 0u;
+                const uint32_t ti = warp_inclusive_scan(t);
+                if (lane < kRsWarps) scan_tmp[lane] = ti - t;
+            }
+            __syncthreads();
+            tile_off[tid] = scan_tmp[warp] + incl - x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kRsIPT; ++j) {
+            if (dig[j] < kRadix) {
+                const uint32_t pos = tile_off[dig[j]] + warp_cnt[warp][dig[j]] + rank[j];
+                stage[pos] = e[j];
+                if constexpr (PAY) stage_pay[pos] = p[j];
+            }
+        }
+        __syncthreads();
+        const uint32_t count = static_cast<uint32_t>(hi - tb < kRsTile ? hi - tb : kRsTile);
+        for (uint32_t q = tid; q < count; q += blockDim.x) {
+            const uint64_t x = stage[q];
+            const uint32_t d = static_cast<uint32_t>((x >> shift) & (kRadix - 1));
+            const uint32_t g = running[d] + (q - tile_off[d]);
+            dst[g] = x;
+            if constexpr (PAY) dst_pay[g] = stage_pay[q];
+        }
+        __syncthreads();
+        if (tid < kRadix) running[tid] += tot[tid];
+        __syncthreads();
+    }
+}
+
+// start[s] = first index of segment s in the segment-sorted entries, s in [0, nseg];
+// start[nseg] = m.
+// Each thread owns 8 consecutive positions k (one load per entry plus the
+// predecessor of its first); positions run to k == m inclusive.
+static __global__ void k_seg_bounds(const uint64_t* ent, uint64_t n, const unsigned long long* n_dev, int seg_shift,
+                                    uint64_t nseg, uint32_t* start) {
+    constexpr int U = 8;
+    const uint64_t m = item_count(n, n_dev);
+    for (uint64_t k0 = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) * U; k0 <= m;
+         k0 += static_cast<uint64_t>(gridDim.x) * blockDim.x * U) {
+        int64_t seg[U + 1];
+        seg[0] = k0 == 0 ? -1 : static_cast<int64_t>(ent[k0 - 1] >> seg_shift);
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint64_t k = k0 + j;
+            seg[j + 1] = k < m ? static_cast<int64_t>(ent[k] >> seg_shift) : static_cast<int64_t>(nseg);
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint64_t k = k0 + j;
+            if (k > m) break;
+            for (int64_t s = seg[j] + 1; s <= seg[j + 1]; ++s) start[s] = static_cast<uint32_t>(k);
+        }
+    }
+}
+
+enum SegOp : int { SEG_INSERT = 0, SEG_CONTAINS = 1, SEG_DELETE = 2 };
+
+// Shared-memory segment pass.  round 1: entries carry the primary bucket;
+// misses are appended (keyed by the alternate bucket) to `next`.  round 2:
+// entries carry the alternate bucket; insert misses are appended to `next`
+// for eviction, lookup/delete misses are final.  Hits set bit `payload` of
+// `bitmap` when a bitmap is given.
+template <class C, int OP>
+__global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t* ent, const uint32_t* pay,
+                                                     const uint32_t* start, uint64_t nseg, int sb_log2, int round,
+                                                     uint64_t* next, uint32_t* next_pay,
+                                                     unsigned long long* next_count, uint32_t* bitmap) {
+    extern __shared__ __align__(16) uint64_t seg[];
+    __shared__ uint32_t s_warp[32];
+    __shared__ unsigned long long s_base;
+    constexpr int WPB = C::bucket_bytes / 8;  // 64-bit words per bucket
+    const uint64_t sb = 1ull << sb_log2;
+    const uint32_t seg_words = static_cast<uint32_t>(sb * WPB);
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    uint32_t n_ok = 0;
+    bool err = false;
+    for (uint64_t s = blockIdx.x; s < nseg; s += gridDim.x) {
+        const uint32_t lo = start[s], hi = start[s + 1];
+        if (lo == hi) continue;
+        uint64_t* gseg = reinterpret_cast<uint64_t*>(t.buckets + (s << sb_log2) * C::bucket_bytes);
+        if (seg_words % 2 == 0) {
+            // 16-byte streaming loads, 8 per thread in flight
+            const ulonglong2* g2 = reinterpret_cast<const ulonglong2*>(gseg);
+            ulonglong2* s2 = reinterpret_cast<ulonglong2*>(seg);
+            const uint32_t pairs = seg_words / 2;
+            for (uint32_t w0 = tid; w0 < pairs; w0 += blockDim.x * 8) {
+                ulonglong2 v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (w0 + j * blockDim.x < pairs) v[j] = __ldcs(g2 + w0 + j * blockDim.x);
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (w0 + j * blockDim.x < pairs) s2[w0 + j * blockDim.x] = v[j];
+            }
+        } else {  // a one-word table
+            for (uint32_t w = tid; w < seg_words; w += blockDim.x) seg[w] = gseg[w];
+        }
+        __syncthreads();
+        constexpr int U = 8;  // entries per thread in flight
+        for (uint32_t base = lo; base < hi; base += blockDim.x * U) {
+          uint64_t ev[U];
+          uint32_t pv[U];
+#pragma unroll
+          for (int j = 0; j < U; ++j) {
+              const uint32_t k = base + j * blockDim.x + tid;
+              ev[j] = 0;
+              pv[j] = 0;
+              if (k < hi) {
+                  ev[j] = ent[k];
+                  if (pay) pv[j] = pay[k];
+              }
+          }
+          uint32_t fwd_mask = 0;
+#pragma unroll
+          for (int j = 0; j < U; ++j) {
+            const uint32_t k = base + j * blockDim.x + tid;
+            const bool v = k < hi;
+            bool ok = false;
+            const uint64_t e = ev[j];
+            const uint32_t p = pv[j];
+            if (v) {
+                const uint32_t fp = static_cast<uint32_t>(e) & C::tag_mask;
+                const uint64_t lb = (e >> C::bits) & (sb - 1);
+                uint64_t* bw = seg + lb * WPB;
+                uint64_t c[C::nchunks];
+#pragma unroll
+                for (int q = 0; q < C::nchunks; ++q) c[q] = bw[q];
+                if constexpr (OP == SEG_INSERT)
+                    ok = try_insert<C>(bw, c, fp, err);
+                else if constexpr (OP == SEG_CONTAINS)
+                    ok = has_tag<C>(c, fp);
+                else
+                    ok = try_remove<C>(bw, c, fp, err);
+                if (ok && bitmap) atomicOr(&bitmap[p >> 5], 1u << (p & 31));
+            }
+            n_ok += ok ? 1u : 0u;
+            // misses go to the next round (all of them in round 1; only inserts in round 2)
+            if (v && !ok && (round == 1 || OP == SEG_INSERT)) fwd_mask |= 1u << j;
+          }
+          // one reservation per CTA and step: block-wide prefix sum of the forwards
+          const uint32_t cnt = __popc(fwd_mask);
+          const uint32_t incl = warp_inclusive_scan(cnt);
+          if (lane == 31) s_warp[tid >> 5] = incl;
+          __syncthreads();
+          if (tid < 32) {
+              const uint32_t x = tid < (blockDim.x >> 5) ? s_warp[tid] : 0u;
+              const uint32_t xi = warp_inclusive_scan(x);
+              if (tid < (blockDim.x >> 5)) s_warp[tid] = xi - x;
+              if (tid == 31 && xi) s_base = atomicAdd(next_count, static_cast<unsigned long long>(xi));
+          }
+          __syncthreads();
+          if (fwd_mask) {
+              uint64_t o = s_base + s_warp[tid >> 5] + incl - cnt;
+#pragma unroll
+              for (int j = 0; j < U; ++j) {
+                  if ((fwd_mask >> j) & 1u) {
+                      const uint64_t e = ev[j];
+                      const uint32_t fp = static_cast<uint32_t>(e) & C::tag_mask;
+                      uint64_t b = e >> C::bits;
+                      if (round == 1) b = alt_bucket<C>(b, fp, t.nb_mask);  // keyed by the alternate bucket
+                      next[o] = pack_entry<C>(b, fp);
+                      if (pay) next_pay[o] = pv[j];
+                      ++o;
+                  }
+              }
+          }
+          __syncthreads();  // s_warp / s_base reused by the next step
+        }
+        __syncthreads();
+        if constexpr (OP != SEG_CONTAINS) {
+            if (seg_words % 2 == 0) {
+                ulonglong2* g2 = reinterpret_cast<ulonglong2*>(gseg);
+                const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(seg);
+                for (uint32_t w = tid; w < seg_words / 2; w += blockDim.x) __stcs(g2 + w, s2[w]);
+            } else {
+                for (uint32_t w = tid; w < seg_words; w += blockDim.x) gseg[w] = seg[w];
+            }
+        }
+        __syncthreads();
+    }
+    if constexpr (OP == SEG_INSERT) {
+        flush_counter(&t.ctr[round == 1 ? CTR_PRIMARY : CTR_SECONDARY], n_ok);
+        flush_counter(&t.ctr[CTR_OCCUPIED], n_ok);
+    } else if constexpr (OP == SEG_DELETE) {
+        const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, n_ok);
+        if (lane == 0 && s) {
+            atomicAdd(&t.ctr[CTR_REMOVED], static_cast<unsigned long long>(s));
+            atomicAdd(&t.ctr[CTR_OCCUPIED], ~static_cast<unsigned long long>(s) + 1ull);
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// BFS for a list of keys whose two buckets were full (entries carry (alternate
+// bucket, tag)), eight lanes per key.  Lane j of a key's group reads candidate
+// j of the start bucket (slot (fp + 7j) & (bs-1)) and loads that candidate's
+// alternate bucket, so all candidates' buckets are fetched in one round trip;
+// the candidates with room are then tried in the reference's order
+// (CuckooFilter.cuh:967-1018): copy the candidate to its alternate bucket, swap
+// fp into its slot if it is still there, else undo the copy.  Keys whose
+// candidates all fail are appended to `dfs` for the DFS fallback.
+template <class C>
+__global__ void __launch_bounds__(256) k_evict_bfs_coop(DevTable t, const uint64_t* ent, const uint32_t* pay,
+                                                        const unsigned long long* n_dev, uint32_t* bitmap,
+                                                        uint64_t* dfs, uint32_t* dfs_pay,
+                                                        unsigned long long* dfs_count) {
+    constexpr uint32_t NC = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    const uint32_t lane = threadIdx.x & 31, gl = lane & 7, grp = lane >> 3;
+    const uint32_t gmask = 0xFFu << (grp * 8);
+    const uint64_t m = *n_dev;
+    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    const uint64_t wid = blockIdx.x * static_cast<uint64_t>(blockDim.x / 32) + threadIdx.x / 32;
+    uint32_t n_evk = 0, n_ok = 0, n_ev = 0, n_dup = 0;
+    bool err = false;
+    for (uint64_t i0 = wid * 4; i0 < m; i0 += nwarps * 4) {
+        const uint64_t i = i0 + grp;
+        const bool valid = i < m;
+        uint64_t e = 0, start = 0;
+        uint32_t fp = 0;
+        if (valid) {
+            e = ent[i];
+            fp = static_cast<uint32_t>(e) & C::tag_mask;
+            const uint64_t i2 = e >> C::bits;
+            const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
+            start = (fp & 1u) == 0 ? i1 : i2;
+        }
+        uint64_t* sbw = bucket_words<C>(t, start);
+        const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * gl) & (C::bs - 1));
+        const int sw = static_cast<int>(slot / C::tpw);
+        const int sh = static_cast<int>(slot % C::tpw) * C::bits;
+        uint32_t cand = 0;
+        uint64_t ab = 0;
+        bool room = false;
+        if (valid && gl < NC) {
+            uint64_t snap[C::nchunks];
+            load_rlx<C::bucket_bytes>(sbw, snap);
+            cand = static_cast<uint32_t>((pick(snap, sw) >> sh) & lane_mask);
+            if (cand == 0) {
+                room = true;  // an empty start slot: tryInsertAtBucket(start, fp), reference :980-985
+            } else {
+                ab = alt_bucket<C>(start, cand, t.nb_mask);
+                uint64_t c[C::nchunks];
+                load_rlx<C::bucket_bytes>(bucket_words<C>(t, ab), c);
+                uint64_t z = 0;
+#pragma unroll
+                for (int q = 0; q < C::nchunks; ++q) z |= zero_lanes<C::bits>(c[q]);
+                room = z != 0;
+            }
+        }
+        uint32_t todo = __ballot_sync(0xFFFFFFFFu, room) & gmask;
+        int done = 0;
+        while (todo) {  // candidates with room, lowest first (group-uniform)
+            const int leader = __ffs(todo) - 1;
+            int res = 0;
+            if (static_cast<int>(lane) == leader) {
+                uint64_t c[C::nchunks];
+                if (cand == 0) {
+                    load_rlx<C::bucket_bytes>(sbw, c);
+                    res = try_insert<C>(sbw, c, fp, err) ? 1 : 0;
+                } else {
+                    uint64_t* abw = bucket_words<C>(t, ab);
+                    load_rlx<C::bucket_bytes>(abw, c);
+                    if (try_insert<C>(abw, c, cand, err)) {
+                        const uint64_t word = load_word_rlx(sbw + sw);
+                        if (((word >> sh) & lane_mask) == cand) {
+                            const uint64_t desired = (word & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
+                            res = cas64(sbw + sw, word, desired) == word ? 2 : 0;
+                        }
+                        if (!res && !remove_from_pair<C>(t, ab, start, cand, err)) ++n_dup;
+                    }
+                }
+            }
+            res = __shfl_sync(gmask, res, leader);
+            if (res) {
+                done = res;
+                break;
+            }
+            todo &= ~(1u << leader);
+        }
+        if (valid && gl == 0) {
+            ++n_evk;
+            if (done) {
+                ++n_ok;
+                if (done == 2) ++n_ev;
+                if (bitmap) atomicOr(&bitmap[pay[i] >> 5], 1u << (pay[i] & 31));
+            } else {
+                const unsigned long long o = atomicAdd(dfs_count, 1ull);
+                dfs[o] = e;
+                if (dfs_pay) dfs_pay[o] = pay[i];
+            }
+        }
+    }
+    flush_counter(&t.ctr[CTR_OCCUPIED], n_ok + n_dup);
+    flush_counter(&t.ctr[CTR_DUP], n_dup);
+    flush_counter(&t.ctr[CTR_EVICTED_INSERTS], n_evk);
+    flush_counter(&t.ctr[CTR_EVICTIONS], n_ev);
+    if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// BFS for a list of keys whose two buckets were full (entries carry (alternate
+// bucket, tag)), as a per-lane step machine.  Every iteration each lane takes
+// one dependent memory step of its current key: read the start bucket, or try
+// the next candidate (load its alternate bucket; if it has room, copy the
+// candidate there and swap fp into its slot, undoing the copy if the slot
+// changed).  A lane whose key is done takes the next key of its warp's share of
+// the list, so no lane waits for a neighbour's longer search.  Candidates are
+// tried in the reference's order (CuckooFilter.cuh:967-1018); keys whose
+// candidates all fail go to `dfs` for the DFS fallback.
+template <class C>
+__global__ void __launch_bounds__(256) k_evict_bfs_steps(DevTable t, const uint64_t* ent, const uint32_t* pay,
+                                                         const unsigned long long* n_dev, uint32_t* bitmap,
+                                                         uint64_t* dfs, uint32_t* dfs_pay,
+                                                         unsigned long long* dfs_count) {
+    constexpr uint32_t NC = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint64_t m = *n_dev;
+    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    const uint64_t wid = blockIdx.x * static_cast<uint64_t>(blockDim.x / 32) + threadIdx.x / 32;
+    const uint64_t per = (m + nwarps - 1) / nwarps;
+    uint64_t next = wid * per;  // warp-uniform cursor into the warp's share
+    const uint64_t end = next + per < m ? next + per : m;
+    uint32_t n_evk = 0, n_ok = 0, n_ev = 0, n_dup = 0;
+    bool err = false;
+    bool has = false, have_snap = false;
+    uint64_t idx = 0, e = 0, start = 0;
+    uint32_t fp = 0, i = 0;
+    uint64_t snap[C::nchunks];
+#pragma unroll
+    for (int q = 0; q < C::nchunks; ++q) snap[q] = 0;
+    for (;;) {
+        const uint32_t need = __ballot_sync(0xFFFFFFFFu, !has);
+        if (need) {
+            if (!has) {
+                const uint64_t k = next + __popc(need & lt_mask);
+                if (k < end) {
+                    has = true;
+                    have_snap = false;
+                    idx = k;
+                    i = 0;
+                    e = ent[k];
+                    fp = static_cast<uint32_t>(e) & C::tag_mask;
+                    const uint64_t i2 = e >> C::bits;
+                    const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
+                    start = (fp & 1u) == 0 ? i1 : i2;
+                    ++n_evk;
+                }
+            }
+            next += __popc(need);
+        }
+        if (__ballot_sync(0xFFFFFFFFu, has) == 0) break;
+        int outcome = 0;  // 1 stored, 2 stored by a swap, 3 candidates exhausted
+        if (has) {
+            uint64_t* sbw = bucket_words<C>(t, start);
+            if (!have_snap) {
+                load_rlx<C::bucket_bytes>(sbw, snap);
+                have_snap = true;
+            } else {
+                const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * i) & (C::bs - 1));
+                const int sw = static_cast<int>(slot / C::tpw);
+                const int sh = static_cast<int>(slot % C::tpw) * C::bits;
+                const uint32_t cand = static_cast<uint32_t>((pick(snap, sw) >> sh) & lane_mask);
+                uint64_t c[C::nchunks];
+                if (cand == 0) {  // reference :980-985
+                    load_rlx<C::bucket_bytes>(sbw, c);
+                    if (try_insert<C>(sbw, c, fp, err)) outcome = 1;
+                } else {
+                    const uint64_t ab = alt_bucket<C>(start, cand, t.nb_mask);
+                    uint64_t* abw = bucket_words<C>(t, ab);
+                    load_rlx<C::bucket_bytes>(abw, c);
+                    if (try_insert<C>(abw, c, cand, err)) {
+                        const uint64_t word = load_word_rlx(sbw + sw);
+                        if (((word >> sh) & lane_mask) == cand) {
+                            const uint64_t desired = (word & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
+                            if (cas64(sbw + sw, word, desired) == word) outcome = 2;
+                        }
+                        if (!outcome) {
+                            if (!remove_from_pair<C>(t, ab, start, cand, err)) ++n_dup;
+                            load_rlx<C::bucket_bytes>(sbw, snap);  // the start bucket changed under us
+                        }
+                    }
+                }
+                if (!outcome && ++i == NC) outcome = 3;
+            }
+        }
+        if (outcome == 1 || outcome == 2) {
+            ++n_ok;
+            if (outcome == 2) ++n_ev;
+            if (bitmap) atomicOr(&bitmap[pay[idx] >> 5], 1u << (pay[idx] & 31));
+        }
+        const uint32_t push = __ballot_sync(0xFFFFFFFFu, outcome == 3);
+        if (push) {
+            unsigned long long base = 0;
+            if (lane == static_cast<uint32_t>(__ffs(push) - 1))
+                base = atomicAdd(dfs_count, static_cast<unsigned long long>(__popc(push)));
+            base = __shfl_sync(0xFFFFFFFFu, base, __ffs(push) - 1);
+            if (outcome == 3) {
+                const uint64_t o = base + __popc(push & lt_mask);
+                dfs[o] = e;
+                if (dfs_pay) dfs_pay[o] = pay[idx];
+            }
+        }
+        if (outcome) has = false;
+        if (err) has = false;  // a retry bound was hit: stop this key, the host reports the error
+    }
+    flush_counter(&t.ctr[CTR_OCCUPIED], n_ok + n_dup);
+    flush_counter(&t.ctr[CTR_DUP], n_dup);
+    flush_counter(&t.ctr[CTR_EVICTED_INSERTS], n_evk);
+    flush_counter(&t.ctr[CTR_EVICTIONS], n_ev);
+    if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// Eviction for the keys whose two buckets were full after both segment rounds
+// (or, with `continued`, whose BFS candidates all failed); entries carry
+// (alternate bucket, tag).  One key per thread, all lanes busy.
+template <class C>
+__global__ void __launch_bounds__(256) k_evict_list(DevTable t, const uint64_t* ent, const uint32_t* pay,
+                                                    const unsigned long long* n_dev, uint32_t policy_bfs,
+                                                    uint32_t max_ev, uint32_t* bitmap, uint32_t continued) {
+    const uint64_t m = *n_dev;
+    uint32_t n_evk = 0, n_fail = 0;
+    EvictStats st;
+    bool err = false;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < m;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t e = ent[i];
+        const uint32_t fp = static_cast<uint32_t>(e) & C::tag_mask;
+        const uint64_t i2 = e >> C::bits;
+        const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
+        const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
+        const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
+        ++n_evk;
+        const bool ok = policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
+                                   : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+        if (ok) {
+            if (bitmap) {
+                const uint32_t p = pay[i];
+                atomicOr(&bitmap[p >> 5], 1u << (p & 31));
+            }
+        } else {
+            ++n_fail;
+        }
+    }
+    flush_counter(&t.ctr[CTR_OCCUPIED], n_evk - n_fail - st.lost + st.dup);
+    flush_counter(&t.ctr[CTR_DUP], st.dup);
+    flush_counter(&t.ctr[CTR_EVICTED_INSERTS], continued ? 0u : n_evk);
+    flush_counter(&t.ctr[CTR_EVICTIONS], st.evictions);
+    flush_counter(&t.ctr[CTR_FAILED], n_fail);
+    flush_counter(&t.ctr[CTR_LOST], st.lost);
+    if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// Round 2 by random access (few keys missed their primary bucket): entries
+// carry (alternate bucket, tag).  insert: first empty slot of the alternate
+// bucket, else eviction; lookup: tag present; delete: remove one copy.
+template <class C, int OP>
+__global__ void __launch_bounds__(256) k_list_random(DevTable t, const uint64_t* ent, const uint32_t* pay,
+                                                     const unsigned long long* n_dev, uint32_t policy_bfs,
+                                                     uint32_t max_ev, uint32_t* bitmap) {
+    const uint64_t m = *n_dev;
+    uint32_t n_sec = 0, n_evk = 0, n_fail = 0;
+    EvictStats st;
+    bool err = false;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < m;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t e = ent[i];
+        const uint32_t fp = static_cast<uint32_t>(e) & C::tag_mask;
+        const uint64_t i2 = e >> C::bits;
+        uint64_t* bw = bucket_words<C>(t, i2);
+        uint64_t c[C::nchunks];
+        bool ok;
+        if constexpr (OP == SEG_CONTAINS) {
+            load_nc<C::bucket_bytes>(bw, c);
+            ok = has_tag<C>(c, fp);
+        } else {
+            load_rlx<C::bucket_bytes>(bw, c);
+            ok = OP == SEG_INSERT ? try_insert<C>(bw, c, fp, err) : try_remove<C>(bw, c, fp, err);
+        }
+        if constexpr (OP == SEG_INSERT) {
+            if (ok) {
+                ++n_sec;
+            } else {
+                const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
+                const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
+                const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
+                ++n_evk;
+                ok = policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
+                                : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+                if (!ok) ++n_fail;
+            }
+        } else if constexpr (OP == SEG_DELETE) {
+            n_sec += ok ? 1u : 0u;
+        }
+        if (ok && bitmap) {
+            const uint32_t p = pay[i];
+            atomicOr(&bitmap[p >> 5], 1u << (p & 31));
+        }
+    }
+    if constexpr (OP == SEG_INSERT) {
+        flush_counter(&t.ctr[CTR_OCCUPIED], n_sec + n_evk - n_fail - st.lost + st.dup);
+        flush_counter(&t.ctr[CTR_DUP], st.dup);
+        flush_counter(&t.ctr[CTR_SECONDARY], n_sec);
+        flush_counter(&t.ctr[CTR_EVICTED_INSERTS], n_evk);
+        flush_counter(&t.ctr[CTR_EVICTIONS], st.evictions);
+        flush_counter(&t.ctr[CTR_FAILED], n_fail);
+        flush_counter(&t.ctr[CTR_LOST], st.lost);
+    } else if constexpr (OP == SEG_DELETE) {
+        const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, n_sec);
+        if ((threadIdx.x & 31) == 0 && s) {
+            atomicAdd(&t.ctr[CTR_REMOVED], static_cast<unsigned long long>(s));
+            atomicAdd(&t.ctr[CTR_OCCUPIED], ~static_cast<unsigned long long>(s) + 1ull);
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// out[i] = bit i of the bitmap, for i < n.
+static __global__ void k_bitmap_expand(const uint32_t* bitmap, uint64_t n, uint8_t* out) {
+    for (uint64_t w = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; w * 32 < n;
+         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t bits = bitmap[w];
+        const uint64_t i0 = w * 32;
+        if (i0 + 32 <= n && (reinterpret_cast<uintptr_t>(out + i0) & 15) == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint64_t lo = 0, hi = 0;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    lo |= static_cast<uint64_t>((bits >> (16 * h + j)) & 1u) << (8 * j);
+                    hi |= static_cast<uint64_t>((bits >> (16 * h + 8 + j)) & 1u) << (8 * j);
+                }
+                asm volatile("st.global.cs.v2.u64 [%0], {%1,%2};" ::"l"(out + i0 + 16 * h), "l"(lo), "l"(hi)
+                             : "memory");
+            }
+        } else {
+            for (uint64_t i = i0; i < n && i < i0 + 32; ++i) out[i] = static_cast<uint8_t>((bits >> (i - i0)) & 1u);
+        }
+    }
+}
+
+}  // namespace cfb

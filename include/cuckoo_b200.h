@@ -82,6 +82,7 @@ typedef struct cf_stats {
     uint64_t failed;          /* inserts that failed (table unchanged for that key) */
     uint64_t lost;            /* stored tags dropped by crossing eviction walks (expected 0) */
     uint64_t removed;         /* successful deletes */
+    uint64_t duplicates;      /* BFS copies left behind by racing walks (an extra entry; expected 0) */
 } cf_stats;
 
 /* Library ABI version (CF_ABI_VERSION). */
@@ -169,6 +170,27 @@ int cf_table(cf_filter* f, void** d_table, uint64_t* bytes);
 /* Replace the table image with `bytes` bytes from `src` (device or host memory)
  * and recount the occupancy.  Synchronous. */
 int cf_load_table(cf_filter* f, const void* src, uint64_t bytes, void* stream);
+
+/* Tunables of a filter (cf_set_option / cf_get_option). */
+typedef enum cf_option {
+    /* Upper bound on the device workspace of the segment-staged path, in bytes
+     * (default 4 GiB).  Larger batches are processed in chunks that fit. */
+    CF_OPT_WORKSPACE_LIMIT = 1,
+    /* Batch size from which containsMany/deleteMany (and the alternate-bucket
+     * round of every segment-staged batch) stream table segments through shared
+     * memory instead of probing at random.  0 = automatic (table bytes / 128 for
+     * lookups, / 64 for inserts and deletes); UINT64_MAX = never. */
+    CF_OPT_SEGMENTED_MIN_KEYS = 2,
+    /* Read-only: bytes of workspace currently allocated. */
+    CF_OPT_WORKSPACE_BYTES = 3,
+    /* Inside a segment-staged batch: number of keys that missed their primary
+     * bucket from which the alternate-bucket round is segment-staged too
+     * (otherwise those keys are probed at random).  0 = automatic, as above. */
+    CF_OPT_ROUND2_SEGMENTED_MIN_KEYS = 4
+} cf_option;
+
+int cf_set_option(cf_filter* f, int option, uint64_t value);
+int cf_get_option(cf_filter* f, int option, uint64_t* value);
 
 /* Copy the table image to `dst` (device or host memory, `bytes` == table size). Synchronous. */
 int cf_store_table(cf_filter* f, void* dst, uint64_t bytes, void* stream);

@@ -211,7 +211,7 @@ def test_bulk_insert_invariants(cfb, orc, kb, bits, bs, policy):
     occ = f.insertMany(d, d_output=ok_t)
     ok = host_u8(ok_t).astype(bool)
     st = f.stats()
-    assert occ == ok.sum() == st["occupied"] == f.countOccupiedSlots()
+    assert occ == ok.sum() == st["occupied"] == f.countOccupiedSlots(), (st, int(ok.sum()), f.countOccupiedSlots())
     assert st["lost"] == 0
     assert st["primary"] + st["secondary"] + st["evicted_inserts"] == len(keys)
     assert st["failed"] == len(keys) - ok.sum()
