@@ -69,6 +69,9 @@ struct OpsTable {
 
 inline bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
 
+// Per-device launch attributes are remembered for device ordinals below this.
+constexpr int kMaxDevices = 64;
+
 // Blocks of `kernel` resident on one SM (at least 1).
 template <class K>
 int blocks_per_sm(K kernel, int threads, size_t smem) {
@@ -192,23 +195,31 @@ struct Launchers {
     template <int OP>
     static cudaError_t seg_round(const DevTable& t, const SegGeom& g, const SegWork& w, int buf, bool payload,
                                  int round, uint64_t n, cudaStream_t s) {
-        static bool attr_set = false;
-        const int smem = static_cast<int>((1ull << g.sb_log2) * C::bucket_bytes);
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(k_seg<C, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSegBytes);
+        // the insert kernel stages a slot mask per bucket beside the segment
+        constexpr int kMaxSmem = OP == SEG_INSERT ? kSegBytes + (kSegBytes / C::bucket_bytes) * sizeof(SlotMask<C>)
+                                                  : kSegBytes;
+        auto kern = OP == SEG_INSERT ? k_seg_insert<C> : k_seg<C, OP>;
+        const int smem = static_cast<int>(OP == SEG_INSERT ? seg_insert_smem<C>(g.sb_log2)
+                                                           : (1ull << g.sb_log2) * C::bucket_bytes);
+        static bool attr_set[kMaxDevices] = {};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+        if (!attr_set[dev]) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
             if (e != cudaSuccess) return e;
-            attr_set = true;
+            attr_set[dev] = true;
         }
         const uint64_t bthreads = n / 8 + 1;  // 8 positions per thread
         const int bgrid = static_cast<int>((bthreads + 255) / 256 < 4096 ? (bthreads + 255) / 256 : 4096);
         k_seg_bounds<<<bgrid, 256, 0, s>>>(w.ent[buf], n, nullptr, g.seg_shift, g.nseg, w.start);
         const int other = 1 - buf;
         // one wave: every resident CTA gets an equal share of the segments
-        static const int bps = blocks_per_sm(k_seg<C, OP>, kSegThreads, kSegBytes);
-        k_seg<C, OP><<<w.sms * bps, kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start,
-                                                           g.nseg, g.sb_log2, round, w.ent[other],
-                                                           payload ? w.pay[other] : nullptr, &w.cnt[round - 1],
-                                                           payload ? w.bitmap : nullptr);
+        static const int bps = blocks_per_sm(kern, kSegThreads, kMaxSmem);
+        kern<<<w.sms * bps, kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start, g.nseg,
+                                                    g.sb_log2, round, w.ent[other], payload ? w.pay[other] : nullptr,
+                                                    &w.cnt[round - 1], payload ? w.bitmap : nullptr);
         return cudaGetLastError();
     }
 

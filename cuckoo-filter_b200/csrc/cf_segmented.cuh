@@ -675,6 +675,174 @@ __global__ void __launch_bounds__(256) k_evict_list(DevTable t, const uint64_t* 
     if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
 }
 
+// Per-bucket empty-slot mask type: one bit per slot.
+template <class C>
+using SlotMask = typename std::conditional<(C::bs > 32), unsigned long long, unsigned int>::type;
+
+// Shared memory of k_seg_insert: the staged segment plus one slot mask per bucket.
+template <class C>
+constexpr size_t seg_insert_smem(int sb_log2) {
+    return (static_cast<size_t>(1) << sb_log2) * (C::bucket_bytes + sizeof(SlotMask<C>));
+}
+
+// Empty-slot mask of a bucket image (bit s set when slot s holds 0).
+template <class C>
+__device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
+    SlotMask<C> m = 0;
+#pragma unroll
+    for (int j = 0; j < C::nchunks; ++j) {
+        const uint64_t z = zero_lanes<C::bits>(bw[j]);
+#pragma unroll
+        for (int l = 0; l < C::lanes_per_chunk; ++l)
+            m |= static_cast<SlotMask<C>>((z >> (l * C::bits + C::bits - 1)) & 1u) << (j * C::lanes_per_chunk + l);
+    }
+    return m;
+}
+
+// Segment-staged insert.  The staged segment carries an empty-slot mask per
+// bucket.  A tag takes the first empty slot circularly from slot
+// align_down(fp & (bs-1), tagsPerWord) -- exactly the order in which the
+// reference's tryInsertAtBucket scans words and lanes (CuckooFilter.cuh:859-904)
+// -- claimed with one compare-and-swap on the mask, then written into the slot
+// with a plain store (the claim makes the slot the thread's own).  Tags whose
+// bucket is full go to `next`: keyed by the alternate bucket in round 1,
+// unchanged (for eviction) in round 2.
+template <class C>
+__global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const uint64_t* ent, const uint32_t* pay,
+                                                            const uint32_t* start, uint64_t nseg, int sb_log2,
+                                                            int round, uint64_t* next, uint32_t* next_pay,
+                                                            unsigned long long* next_count, uint32_t* bitmap) {
+    using M = SlotMask<C>;
+    extern __shared__ __align__(16) uint64_t seg[];
+    __shared__ uint32_t s_warp[32];
+    __shared__ unsigned long long s_base;
+    constexpr int WPB = C::bucket_bytes / 8;
+    constexpr int TB = C::bits / 8;  // tag bytes
+    constexpr M kFull = C::bs == 64 ? ~static_cast<M>(0) : ((static_cast<M>(1) << C::bs) - 1);
+    const uint32_t sb = 1u << sb_log2;
+    const uint32_t seg_words = sb * WPB;
+    M* mask = reinterpret_cast<M*>(seg + seg_words);
+    uint8_t* seg_bytes = reinterpret_cast<uint8_t*>(seg);
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    uint32_t n_ok = 0;
+    for (uint64_t s = blockIdx.x; s < nseg; s += gridDim.x) {
+        const uint32_t lo = start[s], hi = start[s + 1];
+        if (lo == hi) continue;
+        uint64_t* gseg = reinterpret_cast<uint64_t*>(t.buckets + (s << sb_log2) * C::bucket_bytes);
+        if (seg_words % 2 == 0) {
+            const ulonglong2* g2 = reinterpret_cast<const ulonglong2*>(gseg);
+            ulonglong2* s2 = reinterpret_cast<ulonglong2*>(seg);
+            const uint32_t pairs = seg_words / 2;
+            for (uint32_t w0 = tid; w0 < pairs; w0 += blockDim.x * 8) {
+                ulonglong2 v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (w0 + j * blockDim.x < pairs) v[j] = __ldcs(g2 + w0 + j * blockDim.x);
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (w0 + j * blockDim.x < pairs) s2[w0 + j * blockDim.x] = v[j];
+            }
+        } else {
+            for (uint32_t w = tid; w < seg_words; w += blockDim.x) seg[w] = gseg[w];
+        }
+        __syncthreads();
+        for (uint32_t b = tid; b < sb; b += blockDim.x) mask[b] = empty_mask<C>(seg + static_cast<uint64_t>(b) * WPB);
+        __syncthreads();
+        constexpr int U = 8;
+        for (uint32_t base = lo; base < hi; base += blockDim.x * U) {
+            uint64_t ev[U];
+            uint32_t pv[U];
+#pragma unroll
+            for (int j = 0; j < U; ++j) {
+                const uint32_t k = base + j * blockDim.x + tid;
+                ev[j] = 0;
+                pv[j] = 0;
+                if (k < hi) {
+                    ev[j] = ent[k];
+                    if (pay) pv[j] = pay[k];
+                }
+            }
+            uint32_t fwd_mask = 0;
+#pragma unroll
+            for (int j = 0; j < U; ++j) {
+                const uint32_t k = base + j * blockDim.x + tid;
+                if (k >= hi) continue;
+                const uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
+                const uint32_t lb = static_cast<uint32_t>(ev[j] >> C::bits) & (sb - 1);
+                const uint32_t s0 = ((fp & (C::bs - 1)) / C::tpw) * C::tpw;
+                M m = mask[lb];
+                bool ok = false;
+                for (int it = 0; it < 64 && m; ++it) {
+                    // first empty slot circularly from s0
+                    const M rot = s0 ? (((m >> s0) | (m << (C::bs - s0))) & kFull) : m;
+                    uint32_t off;
+                    if constexpr (sizeof(M) == 8)
+                        off = __ffsll(static_cast<long long>(rot)) - 1;
+                    else
+                        off = __ffs(static_cast<int>(rot)) - 1;
+                    const uint32_t slot = (s0 + off) & (C::bs - 1);
+                    const M old = atomicCAS(&mask[lb], m, m & ~(static_cast<M>(1) << slot));
+                    if (old == m) {
+                        uint8_t* dst = seg_bytes + (static_cast<uint64_t>(lb) * C::bucket_bytes + slot * TB);
+                        if constexpr (TB == 1)
+                            *dst = static_cast<uint8_t>(fp);
+                        else if constexpr (TB == 2)
+                            *reinterpret_cast<uint16_t*>(dst) = static_cast<uint16_t>(fp);
+                        else
+                            *reinterpret_cast<uint32_t*>(dst) = fp;
+                        ok = true;
+                        break;
+                    }
+                    m = old;
+                }
+                if (ok) {
+                    ++n_ok;
+                    if (bitmap) atomicOr(&bitmap[pv[j] >> 5], 1u << (pv[j] & 31));
+                } else {
+                    fwd_mask |= 1u << j;
+                }
+            }
+            // one reservation per CTA and step for the tags that found their bucket full
+            const uint32_t cnt = __popc(fwd_mask);
+            const uint32_t incl = warp_inclusive_scan(cnt);
+            if (lane == 31) s_warp[tid >> 5] = incl;
+            __syncthreads();
+            if (tid < 32) {
+                const uint32_t x = tid < (blockDim.x >> 5) ? s_warp[tid] : 0u;
+                const uint32_t xi = warp_inclusive_scan(x);
+                if (tid < (blockDim.x >> 5)) s_warp[tid] = xi - x;
+                if (tid == 31 && xi) s_base = atomicAdd(next_count, static_cast<unsigned long long>(xi));
+            }
+            __syncthreads();
+            if (fwd_mask) {
+                uint64_t o = s_base + s_warp[tid >> 5] + incl - cnt;
+#pragma unroll
+                for (int j = 0; j < U; ++j) {
+                    if ((fwd_mask >> j) & 1u) {
+                        const uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
+                        uint64_t b = ev[j] >> C::bits;
+                        if (round == 1) b = alt_bucket<C>(b, fp, t.nb_mask);
+                        next[o] = pack_entry<C>(b, fp);
+                        if (pay) next_pay[o] = pv[j];
+                        ++o;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (seg_words % 2 == 0) {
+            ulonglong2* g2 = reinterpret_cast<ulonglong2*>(gseg);
+            const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(seg);
+            for (uint32_t w = tid; w < seg_words / 2; w += blockDim.x) __stcs(g2 + w, s2[w]);
+        } else {
+            for (uint32_t w = tid; w < seg_words; w += blockDim.x) gseg[w] = seg[w];
+        }
+        __syncthreads();
+    }
+    flush_counter(&t.ctr[round == 1 ? CTR_PRIMARY : CTR_SECONDARY], n_ok);
+    flush_counter(&t.ctr[CTR_OCCUPIED], n_ok);
+}
+
 // Round 2 by random access (few keys missed their primary bucket): entries
 // carry (alternate bucket, tag).  insert: first empty slot of the alternate
 // bucket, else eviction; lookup: tag present; delete: remove one copy.
