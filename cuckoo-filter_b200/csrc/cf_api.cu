@@ -163,6 +163,8 @@ int finish(cf_filter* f, void* stream, uint64_t* occupied_out) {
     CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
     if (f->h_ctr[CTR_ERROR] & ERR_CAS_LIMIT)
         return fail(CF_ERR_DEVICE, "a compare-and-swap retry bound was hit on the device");
+    if (f->h_ctr[CTR_ERROR] & ERR_WAIT_LIMIT)
+        return fail(CF_ERR_DEVICE, "a bulk copy did not complete within its poll bound on the device");
     if (occupied_out) *occupied_out = f->h_ctr[CTR_OCCUPIED];
     return CF_OK;
 }
@@ -193,9 +195,12 @@ uint64_t ws_need(const cf_filter* f, uint64_t cap, int grid, bool payload) {
 }
 
 int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
-    // radix passes: one wave of the (heaviest) scatter kernel, fixed per-CTA chunks
-    static const int rs_bps = blocks_per_sm(k_rs_scatter<2>, kRsThreads, 0);
-    const int grid = f->sms * rs_bps;
+    // radix passes: one wave of each payload mode's scatter kernel, fixed per-CTA chunks
+    int rs_grid[3];
+    CF_CUDA(rs_scatter_grid<0>(f->sms, &rs_grid[0]), "radix launch setup");
+    CF_CUDA(rs_scatter_grid<1>(f->sms, &rs_grid[1]), "radix launch setup");
+    CF_CUDA(rs_scatter_grid<2>(f->sms, &rs_grid[2]), "radix launch setup");
+    const int grid = std::max(rs_grid[0], std::max(rs_grid[1], rs_grid[2]));
     const uint64_t fixed = ws_need(f, 0, grid, payload) + 4096;
     uint64_t cap = n;
     if (f->ws_limit > fixed) {
@@ -239,7 +244,7 @@ int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     }
     w->h_cnt = f->h_cnt;
     w->cap = cap;
-    w->grid = grid;
+    for (int i = 0; i < 3; ++i) w->rs_grid[i] = rs_grid[i];
     w->sms = f->sms;
     return CF_OK;
 }

@@ -241,4 +241,48 @@ __device__ __forceinline__ void ld_stream_v4u32(const uint32_t* p, uint32_t& a, 
                  : "l"(p));
 }
 
+// ------------------------------------------- bulk copies (TMA) and mbarriers
+//
+// One-dimensional cp.async.bulk global -> shared copies completing on an
+// mbarrier's transaction count.  Source and destination must be 16-byte
+// aligned and the size a multiple of 16 bytes.  No multicast form is used.
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// Makes initialised mbarriers visible to the async proxy (before __syncthreads).
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Orders this thread's earlier generic shared-memory accesses before later
+// async-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Waits until the phase with parity `parity` of `bar` completes.  Returns
+// false after `limit` unsuccessful polls (each poll may suspend the thread for
+// a hardware-defined interval), so a copy that never lands cannot hang the CTA.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    const uint32_t a = smem_addr(bar);
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+constexpr uint32_t kMbarPollLimit = 1u << 22;
+
 }  // namespace cfb

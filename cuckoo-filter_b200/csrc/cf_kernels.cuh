@@ -50,7 +50,8 @@ enum Counter : int {
     CTR_DUP = 9,
     CTR_COUNT = 16
 };
-constexpr uint64_t ERR_CAS_LIMIT = 1;
+constexpr uint64_t ERR_CAS_LIMIT = 1;   // a compare-and-swap retry bound was hit
+constexpr uint64_t ERR_WAIT_LIMIT = 2;  // a bulk copy did not complete within its poll bound
 
 struct DevTable {
     uint8_t* buckets;

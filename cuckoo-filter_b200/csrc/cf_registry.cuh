@@ -28,13 +28,13 @@ struct SegGeom {
 struct SegWork {
     uint64_t* ent[2];
     uint32_t* pay[2];
-    uint32_t* hist;   // kRadix * grid
+    uint32_t* hist;   // kRadix * max(rs_grid)
     uint32_t* start;  // nseg + 1
     unsigned long long* cnt;   // [2] list lengths
     unsigned long long* h_cnt; // pinned mirror
     uint32_t* bitmap;          // cap / 32 words
     uint64_t cap;
-    int grid;      // radix CTAs (one wave of the scatter kernel)
+    int rs_grid[3];  // radix CTAs per payload mode (one wave of that scatter kernel)
     int sms;       // streaming multiprocessors
     uint64_t round2_segmented_min;  // list length from which round 2 is segment-staged
 };
@@ -72,12 +72,38 @@ inline bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintp
 // Per-device launch attributes are remembered for device ordinals below this.
 constexpr int kMaxDevices = 64;
 
+// Raises the dynamic shared-memory limit of `Kernel` to `bytes`, once per device.
+template <auto Kernel>
+cudaError_t ensure_smem_attr(int bytes) {
+    static bool set[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (!set[dev]) {
+        e = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+        set[dev] = true;
+    }
+    return cudaSuccess;
+}
+
 // Blocks of `kernel` resident on one SM (at least 1).
 template <class K>
 int blocks_per_sm(K kernel, int threads, size_t smem) {
     int bps = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, smem) != cudaSuccess || bps < 1) bps = 1;
     return bps;
+}
+
+// CTAs in one wave of the radix scatter for payload mode PAY.
+template <int PAY>
+cudaError_t rs_scatter_grid(int sms, int* grid) {
+    cudaError_t e = ensure_smem_attr<k_rs_scatter<PAY>>(rs_scatter_smem<PAY>());
+    if (e != cudaSuccess) return e;
+    static const int bps = blocks_per_sm(k_rs_scatter<PAY>, kRsThreads, rs_scatter_smem<PAY>());
+    *grid = sms * bps;
+    return cudaSuccess;
 }
 
 inline int grid_for(uint64_t n, int block, int kpt, int max_grid) {
@@ -144,76 +170,91 @@ struct Launchers {
         }
     }
 
-    // One radix pass: items [0, n) of `src` (keys when keys_mode) scattered by
-    // digit `shift` into dst.
-    // One radix pass over n items.  keys_mode: `src` is the key array; the
-    // histogram kernel hashes each key once and writes its packed entry to
-    // ent[1], which the scatter then reads (payload = the key's position).
-    // Otherwise `src` is ent[from] with payloads pay[from].  Scatters to ent[dst].
+    // One radix pass over n items, scattered by the digit at `shift` into
+    // ent[dst].  keys_mode: `src` is the key array; the histogram kernel hashes
+    // each key once and writes its packed entry to ent[1], which the scatter
+    // then reads (payload = the key's position).  Otherwise `src` is ent[from]
+    // with payloads pay[from].  lo_bits >= 0 (the last pass, after passes that
+    // ordered the items by the lower lo_bits bits of the segment id): the
+    // histogram kernel also adds every item's segment into w.start.
     static cudaError_t rs_pass(bool keys_mode, bool payload, const DevTable& t, const void* src, int from, uint64_t n,
-                               int shift, int dst, const SegWork& w, cudaStream_t s) {
-        const uint32_t hist_n = static_cast<uint32_t>(kRadix) * static_cast<uint32_t>(w.grid);
-        const uint64_t* ent_src;
-        if (keys_mode) {
-            k_rs_hist<C, true><<<w.grid, kRsThreads, 0, s>>>(src, t.nb_mask, n, nullptr, shift, w.hist, w.ent[1]);
-            ent_src = w.ent[1];
-        } else {
-            ent_src = w.ent[from];
-            k_rs_hist<C, false><<<w.grid, kRsThreads, 0, s>>>(ent_src, t.nb_mask, n, nullptr, shift, w.hist, nullptr);
-        }
-        k_scan_u32<<<1, 1024, 0, s>>>(w.hist, hist_n);
-        if (!payload)
-            k_rs_scatter<0><<<w.grid, kRsThreads, 0, s>>>(ent_src, nullptr, n, nullptr, shift, w.hist, w.ent[dst],
-                                                          nullptr);
+                               int shift, int dst, const SegWork& w, cudaStream_t s, int lo_bits) {
+        const int pay = !payload ? 0 : keys_mode ? 1 : 2;
+        const int grid = w.rs_grid[pay];
+        const uint32_t hist_n = static_cast<uint32_t>(kRadix) * static_cast<uint32_t>(grid);
+        const uint64_t* ent_src = keys_mode ? w.ent[1] : w.ent[from];
+        const void* hsrc = keys_mode ? src : static_cast<const void*>(ent_src);
+        uint64_t* hout = keys_mode ? w.ent[1] : nullptr;
+        if (keys_mode && lo_bits >= 0)
+            k_rs_hist<C, true, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
+                                                                     lo_bits, w.start);
         else if (keys_mode)
-            k_rs_scatter<1><<<w.grid, kRsThreads, 0, s>>>(ent_src, nullptr, n, nullptr, shift, w.hist, w.ent[dst],
-                                                          w.pay[dst]);
+            k_rs_hist<C, true, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
+                                                                      0, nullptr);
+        else if (lo_bits >= 0)
+            k_rs_hist<C, false, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
+                                                                      nullptr, lo_bits, w.start);
         else
-            k_rs_scatter<2><<<w.grid, kRsThreads, 0, s>>>(ent_src, w.pay[from], n, nullptr, shift, w.hist,
-                                                          w.ent[dst], w.pay[dst]);
+            k_rs_hist<C, false, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
+                                                                       nullptr, 0, nullptr);
+        k_scan_u32<<<1, 1024, 0, s>>>(w.hist, hist_n);
+        unsigned long long* err = t.ctr + CTR_ERROR;
+        if (pay == 0)
+            k_rs_scatter<0><<<grid, kRsThreads, rs_scatter_smem<0>(), s>>>(ent_src, nullptr, n, nullptr, shift, w.hist,
+                                                                          w.ent[dst], nullptr, err);
+        else if (pay == 1)
+            k_rs_scatter<1><<<grid, kRsThreads, rs_scatter_smem<1>(), s>>>(ent_src, nullptr, n, nullptr, shift, w.hist,
+                                                                          w.ent[dst], w.pay[dst], err);
+        else
+            k_rs_scatter<2><<<grid, kRsThreads, rs_scatter_smem<2>(), s>>>(ent_src, w.pay[from], n, nullptr, shift,
+                                                                          w.hist, w.ent[dst], w.pay[dst], err);
         return cudaGetLastError();
     }
 
     // Sort n items by segment id; returns the index of the buffer holding the
     // result.  keys_mode: the source is the key array; otherwise ent/pay[from].
+    // Up to two passes, the last pass also counts the segments, and
+    // *have_start tells that w.start then holds every segment's first index.
     static cudaError_t sort_by_segment(bool keys_mode, bool payload, const DevTable& t, const SegGeom& g,
                                        const SegWork& w, const void* keys, int from, uint64_t n, cudaStream_t s,
-                                       int* result) {
+                                       int* result, bool* have_start) {
         int cur = from;
+        const bool count_segs = g.passes <= 2;
+        if (count_segs) {
+            cudaError_t e = cudaMemsetAsync(w.start, 0, (g.nseg + 1) * sizeof(uint32_t), s);
+            if (e != cudaSuccess) return e;
+        }
         for (int p = 0; p < g.passes; ++p) {
             const bool from_keys = keys_mode && p == 0;
             const int dst = from_keys ? 0 : 1 - cur;
+            const int lo_bits = count_segs && p == g.passes - 1 ? kRadixBits * p : -1;
             cudaError_t e = rs_pass(from_keys, payload, t, from_keys ? keys : nullptr, cur, n,
-                                    g.seg_shift + kRadixBits * p, dst, w, s);
+                                    g.seg_shift + kRadixBits * p, dst, w, s, lo_bits);
             if (e != cudaSuccess) return e;
             cur = dst;
         }
+        if (count_segs) k_scan_u32<<<1, 1024, 0, s>>>(w.start, static_cast<uint32_t>(g.nseg + 1));
         *result = cur;
-        return cudaSuccess;
+        *have_start = count_segs;
+        return cudaGetLastError();
     }
 
     template <int OP>
     static cudaError_t seg_round(const DevTable& t, const SegGeom& g, const SegWork& w, int buf, bool payload,
-                                 int round, uint64_t n, cudaStream_t s) {
+                                 int round, uint64_t n, bool have_start, cudaStream_t s) {
         // the insert kernel stages a slot mask per bucket beside the segment
         constexpr int kMaxSmem = OP == SEG_INSERT ? kSegBytes + (kSegBytes / C::bucket_bytes) * sizeof(SlotMask<C>)
                                                   : kSegBytes;
-        auto kern = OP == SEG_INSERT ? k_seg_insert<C> : k_seg<C, OP>;
+        constexpr auto kern = OP == SEG_INSERT ? k_seg_insert<C> : k_seg<C, OP>;
         const int smem = static_cast<int>(OP == SEG_INSERT ? seg_insert_smem<C>(g.sb_log2)
                                                            : (1ull << g.sb_log2) * C::bucket_bytes);
-        static bool attr_set[kMaxDevices] = {};
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
+        cudaError_t e = ensure_smem_attr<kern>(kMaxSmem);
         if (e != cudaSuccess) return e;
-        if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-        if (!attr_set[dev]) {
-            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-            if (e != cudaSuccess) return e;
-            attr_set[dev] = true;
+        if (!have_start) {
+            const uint64_t bthreads = n / 8 + 1;  // 8 positions per thread
+            const int bgrid = static_cast<int>((bthreads + 255) / 256 < 4096 ? (bthreads + 255) / 256 : 4096);
+            k_seg_bounds<<<bgrid, 256, 0, s>>>(w.ent[buf], n, nullptr, g.seg_shift, g.nseg, w.start);
         }
-        const uint64_t bthreads = n / 8 + 1;  // 8 positions per thread
-        const int bgrid = static_cast<int>((bthreads + 255) / 256 < 4096 ? (bthreads + 255) / 256 : 4096);
-        k_seg_bounds<<<bgrid, 256, 0, s>>>(w.ent[buf], n, nullptr, g.seg_shift, g.nseg, w.start);
         const int other = 1 - buf;
         // one wave: every resident CTA gets an equal share of the segments
         static const int bps = blocks_per_sm(kern, kSegThreads, kMaxSmem);
@@ -230,8 +271,9 @@ struct Launchers {
         cudaError_t e = cudaMemsetAsync(w.cnt, 0, 4 * sizeof(unsigned long long), s);
         if (e == cudaSuccess && payload) e = cudaMemsetAsync(w.bitmap, 0, (m + 31) / 32 * 4, s);
         int a = 0;
-        if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a);
-        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, s);
+        bool have_start = false;
+        if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a, &have_start);
+        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, s);
         // round 2: keys that missed their primary bucket, now in ent/pay[1 - a]
         if (e == cudaSuccess) e = cudaMemcpyAsync(w.h_cnt, w.cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -241,8 +283,8 @@ struct Launchers {
         if (m2 > 0) {
             if (m2 >= w.round2_segmented_min) {
                 int c = b;
-                e = sort_by_segment(false, payload, t, g, w, nullptr, b, m2, s, &c);
-                if (e == cudaSuccess) e = seg_round<OP>(t, g, w, c, payload, 2, m2, s);
+                e = sort_by_segment(false, payload, t, g, w, nullptr, b, m2, s, &c, &have_start);
+                if (e == cudaSuccess) e = seg_round<OP>(t, g, w, c, payload, 2, m2, have_start, s);
                 if (e == cudaSuccess && OP == SEG_INSERT) {
                     // keys whose two buckets are full: ent/pay[1 - c], count cnt[1]
                     uint32_t* bm = payload ? w.bitmap : nullptr;

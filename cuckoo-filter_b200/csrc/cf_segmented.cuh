@@ -37,6 +37,8 @@ constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRsIPT = 8;
 constexpr int kRsTile = kRsThreads * kRsIPT;
+constexpr int kRsHistThreads = 512;
+static_assert(kRsThreads == kRadix, "the scatter's per-digit phases give one thread per digit");
 constexpr int kSegBytes = 65536;
 constexpr int kSegThreads = 256;
 
@@ -71,50 +73,102 @@ __device__ __forceinline__ uint64_t chunk_of(uint64_t n) {
 // Per-CTA digit histogram of its contiguous chunk: hist[digit * grid + cta].
 // KEYS: items are keys, hashed here into packed entries that are also written
 // to `ent_out` (so later passes never hash again); otherwise packed entries.
-template <class C, bool KEYS>
-__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const void* src, uint64_t nb_mask, uint64_t n,
-                                                        const unsigned long long* n_dev, int shift, uint32_t* hist,
-                                                        uint64_t* ent_out) {
+// SEGS (last pass of a sort whose earlier passes ordered the items by the
+// lower `lo_bits` bits of the segment id): also counts every segment,
+// seg_count[(digit << lo_bits) | lower] += 1, so the segment starts are one
+// scan away.  Within a CTA's chunk the lower bits never decrease, so a step of
+// items that all share them is counted in shared memory and flushed when they
+// change; a step that straddles a change counts straight into global memory.
+template <class C, bool KEYS, bool SEGS>
+__global__ void __launch_bounds__(kRsHistThreads, 3)
+    k_rs_hist(const void* src, uint64_t nb_mask, uint64_t n, const unsigned long long* n_dev, int shift,
+              uint32_t* hist, uint64_t* ent_out, int lo_bits, uint32_t* seg_count) {
     __shared__ uint32_t cnt[kRadix];
-    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) cnt[i] = 0;
+    __shared__ uint32_t run_cnt[SEGS ? kRadix : 1];
+    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) {
+        cnt[i] = 0;
+        if constexpr (SEGS) run_cnt[i] = 0;
+    }
     __syncthreads();
     const uint64_t m = item_count(n, n_dev);
     const uint64_t chunk = chunk_of(m);
     const uint64_t lo = blockIdx.x * chunk;
     const uint64_t hi = lo + chunk < m ? lo + chunk : m;
+    const uint64_t* ent = static_cast<const uint64_t*>(src);
+    const int lo_shift = shift - lo_bits;
+    const uint32_t lo_mask = (1u << lo_bits) - 1u;
+    uint32_t cur = 0;  // lower segment bits of the current run (uniform over the CTA)
     constexpr int U = 8;  // independent loads in flight per thread
-    for (uint64_t b = lo; b < hi; b += static_cast<uint64_t>(blockDim.x) * U) {
+    const uint64_t step = static_cast<uint64_t>(blockDim.x) * U;
+    for (uint64_t b = lo; b < hi; b += step) {
+        bool straddle = false;
+        if constexpr (SEGS) {
+            // (a first pass over keys is also the last only when there are no lower bits)
+            uint32_t lf = 0, ll = 0;
+            if (!KEYS && lo_bits > 0) {
+                const uint64_t last = (b + step < hi ? b + step : hi) - 1;
+                lf = static_cast<uint32_t>(ent[b] >> lo_shift) & lo_mask;
+                ll = static_cast<uint32_t>(ent[last] >> lo_shift) & lo_mask;
+            }
+            if (lf != cur) {
+                __syncthreads();
+                for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+                    if (run_cnt[d]) atomicAdd(&seg_count[(static_cast<uint32_t>(d) << lo_bits) | cur], run_cnt[d]);
+                    run_cnt[d] = 0;
+                }
+                __syncthreads();
+                cur = lf;
+            }
+            straddle = lf != ll;
+        }
         uint64_t e[U];
 #pragma unroll
         for (int j = 0; j < U; ++j) {
             const uint64_t i = b + static_cast<uint64_t>(j) * blockDim.x + threadIdx.x;
             e[j] = 0;
-            if (i < hi) e[j] = KEYS ? key_entry<C>(src, i, nb_mask) : static_cast<const uint64_t*>(src)[i];
+            if (i < hi) e[j] = KEYS ? key_entry<C>(src, i, nb_mask) : ent[i];
         }
 #pragma unroll
         for (int j = 0; j < U; ++j) {
             const uint64_t i = b + static_cast<uint64_t>(j) * blockDim.x + threadIdx.x;
             if (i < hi) {
-                atomicAdd(&cnt[(e[j] >> shift) & (kRadix - 1)], 1u);
+                const uint32_t d = static_cast<uint32_t>(e[j] >> shift) & (kRadix - 1);
+                atomicAdd(&cnt[d], 1u);
                 if constexpr (KEYS) ent_out[i] = e[j];
+                if constexpr (SEGS) {
+                    if (!straddle)
+                        atomicAdd(&run_cnt[d], 1u);
+                    else
+                        atomicAdd(&seg_count[(d << lo_bits) | (static_cast<uint32_t>(e[j] >> lo_shift) & lo_mask)], 1u);
+                }
             }
         }
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x] = cnt[d];
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+        hist[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x] = cnt[d];
+        if constexpr (SEGS)
+            if (run_cnt[d]) atomicAdd(&seg_count[(static_cast<uint32_t>(d) << lo_bits) | cur], run_cnt[d]);
+    }
 }
 
-// Exclusive scan of `count` uint32 values in place (one CTA of 1024 threads).
+// Exclusive scan of `count` uint32 values in place (one CTA of 1024 threads,
+// four consecutive values per thread per step).
 static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t count) {
     __shared__ uint32_t warp_tot[32];
     __shared__ uint32_t carry;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (uint32_t base = 0; base < count; base += 1024) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t x = i < count ? v[i] : 0u;
-        const uint32_t incl = warp_inclusive_scan(x);
+    for (uint32_t base = 0; base < count; base += 4096) {
+        const uint32_t i0 = base + threadIdx.x * 4;
+        uint32_t x[4], s = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            x[j] = i0 + j < count ? v[i0 + j] : 0u;
+            s += x[j];
+        }
+        const uint32_t incl = warp_inclusive_scan(s);
         if (lane == 31) warp_tot[warp] = incl;
         __syncthreads();
         if (warp == 0) {
@@ -122,132 +176,181 @@ static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t 
             warp_tot[lane] = warp_inclusive_scan(t) - t;
         }
         __syncthreads();
-        const uint32_t excl = carry + warp_tot[warp] + incl - x;
-        if (i < count) v[i] = excl;
+        uint32_t run = carry + warp_tot[warp] + incl - s;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (i0 + j < count) v[i0 + j] = run;
+            run += x[j];
+        }
         __syncthreads();
-        if (threadIdx.x == 1023) carry = excl + x;
+        if (threadIdx.x == 1023) carry = run;
         __syncthreads();
     }
 }
 
+// Shared memory of k_rs_scatter.
+template <int PAY>
+struct RsScatterSmem {
+    uint64_t in[2][kRsTile];                      // bulk-copy double buffer (entries)
+    uint32_t in_pay[2][PAY == 2 ? kRsTile : 4];   // bulk-copy double buffer (payloads)
+    uint64_t stage[kRsTile];                      // the tile in digit order
+    uint32_t stage_pay[PAY ? kRsTile : 1];
+    uint32_t warp_cnt[kRsWarps][kRadix];          // per-warp digit counts, then their warp prefix
+    uint32_t running[kRadix];                     // next output position per digit
+    uint32_t tot[kRadix];                         // tile count per digit
+    uint32_t tile_off[kRadix];                    // digit offset in the tile, within its group of 32 digits
+    uint32_t grp_off[kRadix / 32];                // offset of each group of 32 digits
+    uint64_t bar[2];
+};
+
 // One stable LSD pass over packed entries: scatter them to dst by digit, using
-// the scanned histogram as the CTA's starting offset per digit.  Each
-// 2048-entry tile is ranked in shared memory (lanes with equal digits found by
-// eight ballots, then warp order, then tile order), staged in digit order, and
-// written out as contiguous runs.  PAY: 0 = no payload, 1 = the payload of
-// entry i is i itself, 2 = payloads read from src_pay.
+// the scanned histogram as the CTA's starting offset per digit.  Full
+// 2048-entry tiles arrive by bulk copy into a double buffer (the copy of tile
+// t+2 is issued as soon as tile t has been read), so the DRAM reads run ahead
+// of the ranking.  Each tile is ranked in shared memory (lanes with equal
+// digits found by one match, then warp order, then tile order), staged in
+// digit order, and written out as contiguous runs.  PAY: 0 = no payload, 1 =
+// the payload of entry i is i itself, 2 = payloads read from src_pay.
 template <int PAY>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __restrict__ src,
                                                            const uint32_t* __restrict__ src_pay, uint64_t n,
                                                            const unsigned long long* n_dev, int shift,
                                                            const uint32_t* offs, uint64_t* __restrict__ dst,
-                                                           uint32_t* __restrict__ dst_pay) {
-    __shared__ uint32_t running[kRadix];
-    __shared__ uint32_t tot[kRadix];
-    __shared__ uint32_t tile_off[kRadix];
-    __shared__ uint32_t warp_cnt[kRsWarps][kRadix];
-    __shared__ uint32_t scan_tmp[kRsWarps];
-    __shared__ uint64_t stage[kRsTile];
-    __shared__ uint32_t stage_pay[PAY ? kRsTile : 1];
+                                                           uint32_t* __restrict__ dst_pay, unsigned long long* err) {
+    extern __shared__ __align__(128) unsigned char rs_raw[];
+    RsScatterSmem<PAY>& sm = *reinterpret_cast<RsScatterSmem<PAY>*>(rs_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint64_t m = item_count(n, n_dev);
     const uint64_t chunk = chunk_of(m);
     const uint64_t lo = blockIdx.x * chunk;
     const uint64_t hi = lo + chunk < m ? lo + chunk : m;
-    for (int d = tid; d < kRadix; d += blockDim.x) running[d] = offs[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x];
-    for (uint64_t tb = lo; tb < hi; tb += kRsTile) {
-        for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&warp_cnt[0][0])[i] = 0;
-        __syncthreads();
+    const uint32_t ntile = lo < hi ? static_cast<uint32_t>((hi - lo + kRsTile - 1) / kRsTile) : 0u;
+    const uint32_t nfull = lo < hi ? static_cast<uint32_t>((hi - lo) / kRsTile) : 0u;  // only the last can be partial
+    for (int d = tid; d < kRadix; d += blockDim.x) {
+        sm.running[d] = offs[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x];
+        sm.tot[d] = 0;
+    }
+    for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&sm.warp_cnt[0][0])[i] = 0;
+    if (tid == 0) {
+        mbar_init(&sm.bar[0], 1);
+        mbar_init(&sm.bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    // thread 0: start the copy of full tile t into buffer t & 1
+    auto issue = [&](uint32_t t) {
+        if (t >= nfull) return;
+        const uint32_t b = t & 1u;
+        const uint64_t i0 = lo + static_cast<uint64_t>(t) * kRsTile;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&sm.bar[b], kRsTile * 8u + (PAY == 2 ? kRsTile * 4u : 0u));
+        bulk_g2s(sm.in[b], src + i0, kRsTile * 8u, &sm.bar[b]);
+        if constexpr (PAY == 2) bulk_g2s(sm.in_pay[b], src_pay + i0, kRsTile * 4u, &sm.bar[b]);
+    };
+    if (tid == 0) {
+        issue(0);
+        issue(1);
+    }
+    bool failed = false;
+    for (uint32_t t = 0; t < ntile; ++t) {
+        const uint32_t b = t & 1u;
+        const uint64_t tb = lo + static_cast<uint64_t>(t) * kRsTile;
+        const bool full = t < nfull;
         uint64_t e[kRsIPT];
-        uint32_t p[kRsIPT];
-        uint32_t rank[kRsIPT];
-        uint32_t dig[kRsIPT];
-        // all loads of the tile first, so they are in flight together
+        uint32_t p[kRsIPT], rank[kRsIPT], dig[kRsIPT];
+        __syncthreads();  // the previous tile's write-out and counter reset are done
+        if (full) {
+            if (!mbar_wait(&sm.bar[b], (t >> 1) & 1u, kMbarPollLimit)) failed = true;
 #pragma unroll
-        for (int j = 0; j < kRsIPT; ++j) {
-            const uint64_t i = tb + warp * 32 * kRsIPT + j * 32 + lane;
-            e[j] = 0;
-            p[j] = 0;
-            if (i < hi) {
-                e[j] = __ldcs(reinterpret_cast<const unsigned long long*>(src) + i);
-                if constexpr (PAY == 1) p[j] = static_cast<uint32_t>(i);
-                if constexpr (PAY == 2) p[j] = __ldcs(reinterpret_cast<const unsigned int*>(src_pay) + i);
+            for (int j = 0; j < kRsIPT; ++j) {
+                const uint32_t idx = warp * 32 * kRsIPT + j * 32 + lane;
+                e[j] = sm.in[b][idx];
+                p[j] = 0;
+                if constexpr (PAY == 1) p[j] = static_cast<uint32_t>(tb + idx);
+                if constexpr (PAY == 2) p[j] = sm.in_pay[b][idx];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kRsIPT; ++j) {
+                const uint64_t i = tb + warp * 32 * kRsIPT + j * 32 + lane;
+                e[j] = 0;
+                p[j] = 0;
+                if (i < hi) {
+                    e[j] = __ldcs(reinterpret_cast<const unsigned long long*>(src) + i);
+                    if constexpr (PAY == 1) p[j] = static_cast<uint32_t>(i);
+                    if constexpr (PAY == 2) p[j] = __ldcs(reinterpret_cast<const unsigned int*>(src_pay) + i);
+                }
             }
         }
 #pragma unroll
         for (int j = 0; j < kRsIPT; ++j) {
-            const uint64_t i = tb + warp * 32 * kRsIPT + j * 32 + lane;
-            const bool v = i < hi;
-            const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
-            dig[j] = v ? d : kRadix;
-            // lanes holding a valid entry with the same digit
-            uint32_t peers = __ballot_sync(0xFFFFFFFFu, v);
-#pragma unroll
-            for (int b = 0; b < kRadixBits; ++b) {
-                const uint32_t bit = (d >> b) & 1u;
-                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
-                peers &= bit ? bal : ~bal;
-            }
-            const int leader = v ? __ffs(peers) - 1 : static_cast<int>(lane);
+            const bool v = full || tb + warp * 32 * kRsIPT + j * 32 + lane < hi;
+            const uint32_t d = v ? static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1)) : static_cast<uint32_t>(kRadix);
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+            const int leader = __ffs(peers) - 1;
             uint32_t base = 0;
-            if (v && static_cast<int>(lane) == leader) {
-                base = warp_cnt[warp][d];
-                warp_cnt[warp][d] = base + __popc(peers);
+            if (static_cast<int>(lane) == leader && d < kRadix) {
+                base = sm.warp_cnt[warp][d];
+                sm.warp_cnt[warp][d] = base + __popc(peers);
             }
             base = __shfl_sync(0xFFFFFFFFu, base, leader);
             rank[j] = base + __popc(peers & lt_mask);
+            dig[j] = d;
             __syncwarp();
         }
-        __syncthreads();
-        // per digit: exclusive prefix over warps, and the tile total
-        if (tid < kRadix) {
+        __syncthreads();  // tile read and ranked: its buffer may be refilled
+        if (tid == 0) issue(t + 2);
+        // thread d: prefix of digit d over warps, the tile total (the previous
+        // tile's total moves into the running offset), scan within its warp
+        {
             uint32_t s = 0;
 #pragma unroll
             for (int w = 0; w < kRsWarps; ++w) {
-                const uint32_t c = warp_cnt[w][tid];
-                warp_cnt[w][tid] = s;
+                const uint32_t c = sm.warp_cnt[w][tid];
+                sm.warp_cnt[w][tid] = s;
                 s += c;
             }
-            tot[tid] = s;
+            sm.running[tid] += sm.tot[tid];
+            sm.tot[tid] = s;
+            const uint32_t incl = warp_inclusive_scan(s);
+            sm.tile_off[tid] = incl - s;
+            if (lane == 31) sm.grp_off[warp] = incl;
         }
         __syncthreads();
-        // exclusive scan of the tile totals over digits (kRadix == kRsThreads)
-        {
-            const uint32_t x = tot[tid];
-            const uint32_t incl = warp_inclusive_scan(x);
-            if (lane == 31) scan_tmp[warp] = incl;
-            __syncthreads();
-            if (warp == 0) {
-                const uint32_t t = lane < kRsWarps ? scan_tmp[lane] : 0u;
-                const uint32_t ti = warp_inclusive_scan(t);
-                if (lane < kRsWarps) scan_tmp[lane] = ti - t;
-            }
-            __syncthreads();
-            tile_off[tid] = scan_tmp[warp] + incl - x;
+        if (warp == 0) {
+            const uint32_t x = lane < kRadix / 32 ? sm.grp_off[lane] : 0u;
+            const uint32_t xi = warp_inclusive_scan(x);
+            if (lane < kRadix / 32) sm.grp_off[lane] = xi - x;
         }
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < kRsIPT; ++j) {
-            if (dig[j] < kRadix) {
-                const uint32_t pos = tile_off[dig[j]] + warp_cnt[warp][dig[j]] + rank[j];
-                stage[pos] = e[j];
-                if constexpr (PAY) stage_pay[pos] = p[j];
+            const uint32_t d = dig[j];
+            if (d < kRadix) {
+                const uint32_t pos = sm.grp_off[d >> 5] + sm.tile_off[d] + sm.warp_cnt[warp][d] + rank[j];
+                sm.stage[pos] = e[j];
+                if constexpr (PAY) sm.stage_pay[pos] = p[j];
             }
         }
         __syncthreads();
-        const uint32_t count = static_cast<uint32_t>(hi - tb < kRsTile ? hi - tb : kRsTile);
+        const uint32_t count = full ? static_cast<uint32_t>(kRsTile) : static_cast<uint32_t>(hi - tb);
         for (uint32_t q = tid; q < count; q += blockDim.x) {
-            const uint64_t x = stage[q];
+            const uint64_t x = sm.stage[q];
             const uint32_t d = static_cast<uint32_t>((x >> shift) & (kRadix - 1));
-            const uint32_t g = running[d] + (q - tile_off[d]);
+            const uint32_t g = sm.running[d] + (q - sm.grp_off[d >> 5] - sm.tile_off[d]);
             dst[g] = x;
-            if constexpr (PAY) dst_pay[g] = stage_pay[q];
+            if constexpr (PAY) dst_pay[g] = sm.stage_pay[q];
         }
-        __syncthreads();
-        if (tid < kRadix) running[tid] += tot[tid];
-        __syncthreads();
+        for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&sm.warp_cnt[0][0])[i] = 0;
     }
+    if (__any_sync(0xFFFFFFFFu, failed) && lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
+}
+
+// Dynamic shared memory of k_rs_scatter<PAY>.
+template <int PAY>
+constexpr int rs_scatter_smem() {
+    return static_cast<int>(sizeof(RsScatterSmem<PAY>));
 }
 
 // start[s] = first index of segment s in the segment-sorted entries, s in [0, nseg];
@@ -718,7 +821,8 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const
     __shared__ unsigned long long s_base;
     constexpr int WPB = C::bucket_bytes / 8;
     constexpr int TB = C::bits / 8;  // tag bytes
-    constexpr M kFull = C::bs == 64 ? ~static_cast<M>(0) : ((static_cast<M>(1) << C::bs) - 1);
+    constexpr int kMaskBits = 8 * sizeof(M);
+    constexpr M kFull = C::bs == kMaskBits ? ~static_cast<M>(0) : ((static_cast<M>(1) << (C::bs % kMaskBits)) - 1);
     const uint32_t sb = 1u << sb_log2;
     const uint32_t seg_words = sb * WPB;
     M* mask = reinterpret_cast<M*>(seg + seg_words);
