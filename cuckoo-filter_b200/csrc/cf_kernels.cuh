@@ -113,6 +113,24 @@ __device__ bool try_insert(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp,
     return false;
 }
 
+// One step of tryInsertAtBucket: the word index and the compare-and-swap
+// values that store fp in the first empty slot of bucket image c, scanning
+// words from fp's start word.  False when c has no empty slot.
+template <class C>
+__device__ __forceinline__ bool plan_insert(const uint64_t (&c)[C::nchunks], uint32_t fp, int& w, uint64_t& cur,
+                                            uint64_t& desired) {
+    const int sw = static_cast<int>((fp & (C::bs - 1)) / C::tpw);
+    uint32_t words = 0;
+#pragma unroll
+    for (int j = 0; j < C::nchunks; ++j) words |= (zero_lanes<C::bits>(c[j]) != 0 ? 1u : 0u) << j;
+    if (!words) return false;
+    w = first_word<C::wc>(words, sw);
+    cur = pick(c, w);
+    const int lane = lowest_lane<C::bits>(zero_lanes<C::bits>(cur));
+    desired = cur | (static_cast<uint64_t>(fp) << (lane * C::bits));
+    return true;
+}
+
 // tryRemoveAtBucket: clear the first slot holding fp.
 template <class C>
 __device__ bool try_remove(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp, bool& err) {

@@ -174,11 +174,12 @@ struct Launchers {
     // ent[dst].  keys_mode: `src` is the key array; the histogram kernel hashes
     // each key once and writes its packed entry to ent[1], which the scatter
     // then reads (payload = the key's position).  Otherwise `src` is ent[from]
-    // with payloads pay[from].  lo_bits >= 0 (the last pass, after passes that
-    // ordered the items by the lower lo_bits bits of the segment id): the
-    // histogram kernel also adds every item's segment into w.start.
+    // with payloads pay[from].  The items are sorted by the `order_bits`
+    // segment bits below `shift` (the earlier passes' digits), whose order
+    // the scatter keeps.  lo_bits >= 0 (the last pass; lo_bits == order_bits):
+    // the histogram kernel also adds every item's segment into w.start.
     static cudaError_t rs_pass(bool keys_mode, bool payload, const DevTable& t, const void* src, int from, uint64_t n,
-                               int shift, int dst, const SegWork& w, cudaStream_t s, int lo_bits) {
+                               int shift, int order_bits, int dst, const SegWork& w, cudaStream_t s, int lo_bits) {
         const int pay = !payload ? 0 : keys_mode ? 1 : 2;
         const int grid = w.rs_grid[pay];
         const uint32_t hist_n = static_cast<uint32_t>(kRadix) * static_cast<uint32_t>(grid);
@@ -200,14 +201,14 @@ struct Launchers {
         k_scan_u32<<<1, 1024, 0, s>>>(w.hist, hist_n);
         unsigned long long* err = t.ctr + CTR_ERROR;
         if (pay == 0)
-            k_rs_scatter<0><<<grid, kRsThreads, rs_scatter_smem<0>(), s>>>(ent_src, nullptr, n, nullptr, shift, w.hist,
+            k_rs_scatter<0><<<grid, kRsThreads, rs_scatter_smem<0>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
                                                                           w.ent[dst], nullptr, err);
         else if (pay == 1)
-            k_rs_scatter<1><<<grid, kRsThreads, rs_scatter_smem<1>(), s>>>(ent_src, nullptr, n, nullptr, shift, w.hist,
+            k_rs_scatter<1><<<grid, kRsThreads, rs_scatter_smem<1>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
                                                                           w.ent[dst], w.pay[dst], err);
         else
             k_rs_scatter<2><<<grid, kRsThreads, rs_scatter_smem<2>(), s>>>(ent_src, w.pay[from], n, nullptr, shift,
-                                                                          w.hist, w.ent[dst], w.pay[dst], err);
+                                                                          order_bits, w.hist, w.ent[dst], w.pay[dst], err);
         return cudaGetLastError();
     }
 
@@ -229,7 +230,7 @@ struct Launchers {
             const int dst = from_keys ? 0 : 1 - cur;
             const int lo_bits = count_segs && p == g.passes - 1 ? kRadixBits * p : -1;
             cudaError_t e = rs_pass(from_keys, payload, t, from_keys ? keys : nullptr, cur, n,
-                                    g.seg_shift + kRadixBits * p, dst, w, s, lo_bits);
+                                    g.seg_shift + kRadixBits * p, kRadixBits * p, dst, w, s, lo_bits);
             if (e != cudaSuccess) return e;
             cur = dst;
         }

@@ -203,18 +203,27 @@ struct RsScatterSmem {
     uint64_t bar[2];
 };
 
-// One stable LSD pass over packed entries: scatter them to dst by digit, using
-// the scanned histogram as the CTA's starting offset per digit.  Full
-// 2048-entry tiles arrive by bulk copy into a double buffer (the copy of tile
-// t+2 is issued as soon as tile t has been read), so the DRAM reads run ahead
-// of the ranking.  Each tile is ranked in shared memory (lanes with equal
-// digits found by one match, then warp order, then tile order), staged in
-// digit order, and written out as contiguous runs.  PAY: 0 = no payload, 1 =
-// the payload of entry i is i itself, 2 = payloads read from src_pay.
+// One LSD pass over packed entries: scatter them to dst by digit, using the
+// scanned histogram as the CTA's starting offset per digit.  Full 2048-entry
+// tiles arrive by bulk copy into a double buffer (the copy of tile t+2 is
+// issued as soon as tile t has been read), so the DRAM reads run ahead of the
+// ranking.  Each tile is ranked in shared memory, staged in digit order and
+// written out as contiguous runs.
+//
+// The sort only has to group entries by segment, so a pass needs to keep the
+// input order only among entries whose lower `lo_bits` segment bits (the
+// digits of the earlier passes) differ.  The input of a later pass is sorted
+// by those bits, so a tile whose first and last entries agree on them holds a
+// single value: it is ranked with one shared-memory atomic per entry (order
+// within a digit unspecified).  Only a tile spanning several lower values
+// (at most one per value change, so a few hundred per pass) is ranked stably
+// (lanes with equal digits found by eight ballots, then warp order).
+// PAY: 0 = no payload, 1 = the payload of entry i is i itself, 2 = payloads
+// read from src_pay.
 template <int PAY>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __restrict__ src,
                                                            const uint32_t* __restrict__ src_pay, uint64_t n,
-                                                           const unsigned long long* n_dev, int shift,
+                                                           const unsigned long long* n_dev, int shift, int lo_bits,
                                                            const uint32_t* offs, uint64_t* __restrict__ dst,
                                                            uint32_t* __restrict__ dst_pay, unsigned long long* err) {
     extern __shared__ __align__(128) unsigned char rs_raw[];
@@ -227,6 +236,8 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
     const uint64_t hi = lo + chunk < m ? lo + chunk : m;
     const uint32_t ntile = lo < hi ? static_cast<uint32_t>((hi - lo + kRsTile - 1) / kRsTile) : 0u;
     const uint32_t nfull = lo < hi ? static_cast<uint32_t>((hi - lo) / kRsTile) : 0u;  // only the last can be partial
+    const int lo_shift = shift - lo_bits;
+    const uint64_t lo_mask = (1ull << lo_bits) - 1ull;
     for (int d = tid; d < kRadix; d += blockDim.x) {
         sm.running[d] = offs[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x];
         sm.tot[d] = 0;
@@ -257,9 +268,11 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
         const uint32_t b = t & 1u;
         const uint64_t tb = lo + static_cast<uint64_t>(t) * kRsTile;
         const bool full = t < nfull;
+        const uint32_t count = full ? static_cast<uint32_t>(kRsTile) : static_cast<uint32_t>(hi - tb);
         uint64_t e[kRsIPT];
         uint32_t p[kRsIPT], rank[kRsIPT], dig[kRsIPT];
         __syncthreads();  // the previous tile's write-out and counter reset are done
+        uint64_t first, last;
         if (full) {
             if (!mbar_wait(&sm.bar[b], (t >> 1) & 1u, kMbarPollLimit)) failed = true;
 #pragma unroll
@@ -270,6 +283,8 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
                 if constexpr (PAY == 1) p[j] = static_cast<uint32_t>(tb + idx);
                 if constexpr (PAY == 2) p[j] = sm.in_pay[b][idx];
             }
+            first = sm.in[b][0];
+            last = sm.in[b][kRsTile - 1];
         } else {
 #pragma unroll
             for (int j = 0; j < kRsIPT; ++j) {
@@ -282,34 +297,62 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
                     if constexpr (PAY == 2) p[j] = __ldcs(reinterpret_cast<const unsigned int*>(src_pay) + i);
                 }
             }
+            first = src[tb];
+            last = src[hi - 1];
         }
+        // uniform over the CTA
+        const bool stable = lo_bits > 0 && ((first >> lo_shift) & lo_mask) != ((last >> lo_shift) & lo_mask);
+        if (!stable) {
+            // rank = arrival order within the digit, counted in warp_cnt[0]
 #pragma unroll
-        for (int j = 0; j < kRsIPT; ++j) {
-            const bool v = full || tb + warp * 32 * kRsIPT + j * 32 + lane < hi;
-            const uint32_t d = v ? static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1)) : static_cast<uint32_t>(kRadix);
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-            const int leader = __ffs(peers) - 1;
-            uint32_t base = 0;
-            if (static_cast<int>(lane) == leader && d < kRadix) {
-                base = sm.warp_cnt[warp][d];
-                sm.warp_cnt[warp][d] = base + __popc(peers);
+            for (int j = 0; j < kRsIPT; ++j) {
+                const bool v = full || tb + warp * 32 * kRsIPT + j * 32 + lane < hi;
+                const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
+                dig[j] = v ? d : static_cast<uint32_t>(kRadix);
+                rank[j] = v ? atomicAdd(&sm.warp_cnt[0][d], 1u) : 0u;
             }
-            base = __shfl_sync(0xFFFFFFFFu, base, leader);
-            rank[j] = base + __popc(peers & lt_mask);
-            dig[j] = d;
-            __syncwarp();
+        } else {
+            // rank = lane order within the warp's row, rows in order, warps in order
+#pragma unroll
+            for (int j = 0; j < kRsIPT; ++j) {
+                const bool v = full || tb + warp * 32 * kRsIPT + j * 32 + lane < hi;
+                const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
+                uint32_t peers = __ballot_sync(0xFFFFFFFFu, v);
+#pragma unroll
+                for (int k = 0; k < kRadixBits; ++k) {
+                    const uint32_t bit = (d >> k) & 1u;
+                    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+                    peers &= bit ? bal : ~bal;
+                }
+                const int leader = v ? __ffs(peers) - 1 : static_cast<int>(lane);
+                uint32_t base = 0;
+                if (v && static_cast<int>(lane) == leader) {
+                    base = sm.warp_cnt[warp][d];
+                    sm.warp_cnt[warp][d] = base + __popc(peers);
+                }
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                rank[j] = base + __popc(peers & lt_mask);
+                dig[j] = v ? d : static_cast<uint32_t>(kRadix);
+                __syncwarp();
+            }
         }
         __syncthreads();  // tile read and ranked: its buffer may be refilled
         if (tid == 0) issue(t + 2);
-        // thread d: prefix of digit d over warps, the tile total (the previous
-        // tile's total moves into the running offset), scan within its warp
+        // thread d: the tile total of digit d (the previous tile's total moves
+        // into the running offset), per-warp prefixes when ranked stably, and
+        // the scan within its group of 32 digits
         {
             uint32_t s = 0;
+            if (!stable) {
+                s = sm.warp_cnt[0][tid];
+                sm.warp_cnt[0][tid] = 0;
+            } else {
 #pragma unroll
-            for (int w = 0; w < kRsWarps; ++w) {
-                const uint32_t c = sm.warp_cnt[w][tid];
-                sm.warp_cnt[w][tid] = s;
-                s += c;
+                for (int w = 0; w < kRsWarps; ++w) {
+                    const uint32_t c = sm.warp_cnt[w][tid];
+                    sm.warp_cnt[w][tid] = s;
+                    s += c;
+                }
             }
             sm.running[tid] += sm.tot[tid];
             sm.tot[tid] = s;
@@ -328,13 +371,13 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
         for (int j = 0; j < kRsIPT; ++j) {
             const uint32_t d = dig[j];
             if (d < kRadix) {
-                const uint32_t pos = sm.grp_off[d >> 5] + sm.tile_off[d] + sm.warp_cnt[warp][d] + rank[j];
+                uint32_t pos = sm.grp_off[d >> 5] + sm.tile_off[d] + rank[j];
+                if (stable) pos += sm.warp_cnt[warp][d];
                 sm.stage[pos] = e[j];
                 if constexpr (PAY) sm.stage_pay[pos] = p[j];
             }
         }
         __syncthreads();
-        const uint32_t count = full ? static_cast<uint32_t>(kRsTile) : static_cast<uint32_t>(hi - tb);
         for (uint32_t q = tid; q < count; q += blockDim.x) {
             const uint64_t x = sm.stage[q];
             const uint32_t d = static_cast<uint32_t>((x >> shift) & (kRadix - 1));
@@ -342,7 +385,8 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
             dst[g] = x;
             if constexpr (PAY) dst_pay[g] = sm.stage_pay[q];
         }
-        for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&sm.warp_cnt[0][0])[i] = 0;
+        if (stable)
+            for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&sm.warp_cnt[0][0])[i] = 0;
     }
     if (__any_sync(0xFFFFFFFFu, failed) && lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
 }
@@ -625,21 +669,29 @@ __global__ void __launch_bounds__(256) k_evict_bfs_coop(DevTable t, const uint64
 }
 
 // BFS for a list of keys whose two buckets were full (entries carry (alternate
-// bucket, tag)), as a per-lane step machine.  Every iteration each lane takes
-// one dependent memory step of its current key: read the start bucket, or try
-// the next candidate (load its alternate bucket; if it has room, copy the
-// candidate there and swap fp into its slot, undoing the copy if the slot
-// changed).  A lane whose key is done takes the next key of its warp's share of
-// the list, so no lane waits for a neighbour's longer search.  Candidates are
-// tried in the reference's order (CuckooFilter.cuh:967-1018); keys whose
-// candidates all fail go to `dfs` for the DFS fallback.
+// bucket, tag)), as a per-lane step machine that keeps one memory operation
+// of every lane in flight: each iteration every lane issues exactly one load
+// (its next entry, or a bucket) or one compare-and-swap, and only then are the
+// results consumed, so a warp waits for one round trip per iteration however
+// its lanes' keys diverge.  Per key: fetch the entry, snapshot the start
+// bucket (i1 for an even tag, i2 for an odd one), then try the candidates in
+// the reference's order (CuckooFilter.cuh:967-1018): candidate slot empty ->
+// insert fp into the start bucket; else load the candidate's alternate
+// bucket, copy the candidate there if it has room, and swap fp into the
+// candidate's slot if the candidate is still there (else undo the copy and
+// refresh the snapshot).  A failed compare-and-swap retries from the value it
+// returned, as tryInsertAtBucket does.  A lane whose key is done takes the
+// next key of its warp's share of the list.  Keys whose candidates all fail go
+// to `dfs` for the DFS fallback.
 template <class C>
-__global__ void __launch_bounds__(256) k_evict_bfs_steps(DevTable t, const uint64_t* ent, const uint32_t* pay,
+__global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_steps(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                          const unsigned long long* n_dev, uint32_t* bitmap,
                                                          uint64_t* dfs, uint32_t* dfs_pay,
                                                          unsigned long long* dfs_count) {
     constexpr uint32_t NC = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
     constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    // phase = the operation in flight
+    enum : uint32_t { P_FETCH, P_SNAP, P_PROBE, P_INS_ALT, P_SWAP, P_INS_START };
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint64_t m = *n_dev;
@@ -650,12 +702,39 @@ __global__ void __launch_bounds__(256) k_evict_bfs_steps(DevTable t, const uint6
     const uint64_t end = next + per < m ? next + per : m;
     uint32_t n_evk = 0, n_ok = 0, n_ev = 0, n_dup = 0;
     bool err = false;
-    bool has = false, have_snap = false;
-    uint64_t idx = 0, e = 0, start = 0;
-    uint32_t fp = 0, i = 0;
+    bool has = false;
+    uint32_t phase = P_FETCH, fp = 0, i = 0, cand = 0, sh = 0, retries = 0;
+    int sw = 0, w = 0;
+    uint64_t idx = 0, e = 0, start = 0, ab = 0, exp = 0, des = 0;
+    const uint64_t* addr = nullptr;  // load or compare-and-swap target
     uint64_t snap[C::nchunks];
 #pragma unroll
     for (int q = 0; q < C::nchunks; ++q) snap[q] = 0;
+
+    // Picks candidate i (or the next ones) from the snapshot and sets up its
+    // first operation; returns 3 when all candidates are used up.
+    auto select = [&]() -> int {
+        for (; i < NC; ++i) {
+            const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * i) & (C::bs - 1));
+            sw = static_cast<int>(slot / C::tpw);
+            sh = (slot % C::tpw) * C::bits;
+            cand = static_cast<uint32_t>((pick(snap, sw) >> sh) & lane_mask);
+            if (cand == 0) {  // reference :980-985: the slot is free, insert fp into the start bucket
+                if (plan_insert<C>(snap, fp, w, exp, des)) {
+                    phase = P_INS_START;
+                    addr = bucket_words<C>(t, start) + w;
+                    return 0;
+                }
+                continue;
+            }
+            ab = alt_bucket<C>(start, cand, t.nb_mask);
+            phase = P_PROBE;
+            addr = bucket_words<C>(t, ab);
+            return 0;
+        }
+        return 3;
+    };
+
     for (;;) {
         const uint32_t need = __ballot_sync(0xFFFFFFFFu, !has);
         if (need) {
@@ -663,52 +742,99 @@ __global__ void __launch_bounds__(256) k_evict_bfs_steps(DevTable t, const uint6
                 const uint64_t k = next + __popc(need & lt_mask);
                 if (k < end) {
                     has = true;
-                    have_snap = false;
                     idx = k;
+                    phase = P_FETCH;
+                    addr = ent + k;
                     i = 0;
-                    e = ent[k];
-                    fp = static_cast<uint32_t>(e) & C::tag_mask;
-                    const uint64_t i2 = e >> C::bits;
-                    const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
-                    start = (fp & 1u) == 0 ? i1 : i2;
+                    retries = 0;
                     ++n_evk;
                 }
             }
             next += __popc(need);
         }
         if (__ballot_sync(0xFFFFFFFFu, has) == 0) break;
+        // issue: one operation per lane, all in flight before any is consumed
+        uint64_t ld[C::nchunks];
+        uint64_t old = 0;
+        const bool do_fetch = has && phase == P_FETCH;
+        const bool do_load = has && (phase == P_SNAP || phase == P_PROBE);
+        const bool do_cas = has && phase >= P_INS_ALT;
+        if (do_fetch) ld[0] = __ldcs(reinterpret_cast<const unsigned long long*>(addr));
+        if (do_load) load_rlx<C::bucket_bytes>(const_cast<uint64_t*>(addr), ld);
+        if (do_cas) old = cas64(const_cast<uint64_t*>(addr), exp, des);
+        // consume
         int outcome = 0;  // 1 stored, 2 stored by a swap, 3 candidates exhausted
         if (has) {
-            uint64_t* sbw = bucket_words<C>(t, start);
-            if (!have_snap) {
-                load_rlx<C::bucket_bytes>(sbw, snap);
-                have_snap = true;
-            } else {
-                const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * i) & (C::bs - 1));
-                const int sw = static_cast<int>(slot / C::tpw);
-                const int sh = static_cast<int>(slot % C::tpw) * C::bits;
-                const uint32_t cand = static_cast<uint32_t>((pick(snap, sw) >> sh) & lane_mask);
-                uint64_t c[C::nchunks];
-                if (cand == 0) {  // reference :980-985
-                    load_rlx<C::bucket_bytes>(sbw, c);
-                    if (try_insert<C>(sbw, c, fp, err)) outcome = 1;
-                } else {
-                    const uint64_t ab = alt_bucket<C>(start, cand, t.nb_mask);
-                    uint64_t* abw = bucket_words<C>(t, ab);
-                    load_rlx<C::bucket_bytes>(abw, c);
-                    if (try_insert<C>(abw, c, cand, err)) {
-                        const uint64_t word = load_word_rlx(sbw + sw);
-                        if (((word >> sh) & lane_mask) == cand) {
-                            const uint64_t desired = (word & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
-                            if (cas64(sbw + sw, word, desired) == word) outcome = 2;
-                        }
-                        if (!outcome) {
-                            if (!remove_from_pair<C>(t, ab, start, cand, err)) ++n_dup;
-                            load_rlx<C::bucket_bytes>(sbw, snap);  // the start bucket changed under us
+            switch (phase) {
+                case P_FETCH: {
+                    e = ld[0];
+                    fp = static_cast<uint32_t>(e) & C::tag_mask;
+                    const uint64_t i2 = e >> C::bits;
+                    const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
+                    start = (fp & 1u) == 0 ? i1 : i2;
+                    phase = P_SNAP;
+                    addr = bucket_words<C>(t, start);
+                    break;
+                }
+                case P_SNAP:
+#pragma unroll
+                    for (int q = 0; q < C::nchunks; ++q) snap[q] = ld[q];
+                    outcome = select();
+                    break;
+                case P_PROBE:
+                    if (plan_insert<C>(ld, cand, w, exp, des)) {
+                        phase = P_INS_ALT;
+                        addr = bucket_words<C>(t, ab) + w;
+                    } else {
+                        ++i;
+                        outcome = select();
+                    }
+                    break;
+                case P_INS_ALT:
+                    if (old == exp) {  // the candidate is copied: swap fp into its slot
+                        exp = pick(snap, sw);
+                        des = (exp & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
+                        phase = P_SWAP;
+                        addr = bucket_words<C>(t, start) + sw;
+                    } else {  // the bucket changed: load it again
+                        phase = P_PROBE;
+                        addr = bucket_words<C>(t, ab);
+                        if (++retries >= kCasRetryLimit) err = true;
+                    }
+                    break;
+                case P_SWAP:
+                    if (old == exp) {
+                        outcome = 2;
+                    } else if (((old >> sh) & lane_mask) == cand) {  // other slots of the word changed
+                        put(snap, sw, old);
+                        exp = old;
+                        des = (old & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
+                        if (++retries >= kCasRetryLimit) err = true;
+                    } else {  // the candidate moved: undo the copy, refresh the snapshot
+                        if (!remove_from_pair<C>(t, ab, start, cand, err)) ++n_dup;
+                        ++i;
+                        if (i == NC) {
+                            outcome = 3;
+                        } else {
+                            phase = P_SNAP;
+                            addr = bucket_words<C>(t, start);
                         }
                     }
-                }
-                if (!outcome && ++i == NC) outcome = 3;
+                    break;
+                default:  // P_INS_START
+                    if (old == exp) {
+                        outcome = 1;
+                    } else {
+                        put(snap, w, old);
+                        if (plan_insert<C>(snap, fp, w, exp, des)) {
+                            addr = bucket_words<C>(t, start) + w;
+                            if (++retries >= kCasRetryLimit) err = true;
+                        } else {
+                            ++i;
+                            outcome = select();
+                        }
+                    }
+                    break;
             }
         }
         if (outcome == 1 || outcome == 2) {
