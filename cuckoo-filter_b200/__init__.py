@@ -112,6 +112,8 @@ def library() -> C.CDLL:
         "cf_store_table": ([vp, vp, u64, vp], i32),
         "cf_probe_count": ([vp, vp, u64, P64, vp], i32),
         "cf_hash_candidates": ([C.POINTER(_Config), u64, vp, u64, vp, vp, vp], i32),
+        "cf_hash64": ([u32, vp, u64, vp], i32),
+        "cf_alt_buckets": ([C.POINTER(_Config), u64, vp, vp, u64, vp], i32),
         "cf_set_option": ([vp, i32, u64], i32),
         "cf_get_option": ([vp, i32, P64], i32),
     }

@@ -607,6 +607,39 @@ int cf_hash_candidates(const cf_config* cfg, uint64_t num_buckets, const void* h
     return CF_OK;
 }
 
+int cf_hash64(uint32_t value_bytes, const void* h_values, uint64_t n, uint64_t* out) {
+    if (value_bytes != 1 && value_bytes != 2 && value_bytes != 4 && value_bytes != 8)
+        return fail(CF_ERR_INVALID, "value_bytes must be 1, 2, 4 or 8");
+    if (n && (!h_values || !out)) return fail(CF_ERR_INVALID, "values or out is NULL with n > 0");
+    const uint8_t* p = static_cast<const uint8_t*>(h_values);
+    for (uint64_t i = 0; i < n; ++i) {
+        uint64_t v = 0;
+        std::memcpy(&v, p + i * value_bytes, value_bytes);
+        out[i] = value_bytes == 8   ? xxh64_u64(v)
+                 : value_bytes == 4 ? xxh64_u32(static_cast<uint32_t>(v))
+                 : value_bytes == 2 ? xxh64_u16(static_cast<uint32_t>(v))
+                                    : xxh64_u8(static_cast<uint32_t>(v));
+    }
+    return CF_OK;
+}
+
+int cf_alt_buckets(const cf_config* cfg, uint64_t num_buckets, const uint64_t* buckets, const uint32_t* tags,
+                   uint64_t n, uint64_t* out) {
+    if (!cfg) return fail(CF_ERR_INVALID, "config is NULL");
+    if (num_buckets == 0 || (num_buckets & (num_buckets - 1)))
+        return fail(CF_ERR_INVALID, "num_buckets must be a power of two");
+    if (n && (!buckets || !tags || !out)) return fail(CF_ERR_INVALID, "buckets, tags or out is NULL with n > 0");
+    const uint32_t bits = cfg->bits_per_tag;
+    if (bits != 8 && bits != 16 && bits != 32) return fail(CF_ERR_INVALID, "bits_per_tag must be 8, 16 or 32");
+    const uint64_t mask = num_buckets - 1;
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint32_t t = bits == 32 ? tags[i] : (tags[i] & ((1u << bits) - 1u));
+        const uint64_t h = bits == 8 ? xxh64_u8(t) : bits == 16 ? xxh64_u16(t) : xxh64_u32(t);
+        out[i] = buckets[i] ^ (h & mask);
+    }
+    return CF_OK;
+}
+
 int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* primary_hits, void* stream) {
     if (int s = check_batch(f, d_keys, n)) return s;
     if (!primary_hits) return fail(CF_ERR_INVALID, "primary_hits is NULL");

@@ -201,6 +201,16 @@ int cf_store_table(cf_filter* f, void* dst, uint64_t bytes, void* stream);
 int cf_hash_candidates(const cf_config* cfg, uint64_t num_buckets, const void* h_keys, uint64_t n, uint64_t* i1,
                        uint64_t* i2, uint32_t* fp);
 
+/* static hash64(key) (CuckooFilter.cuh:362-364 -> xxhash::xxhash64, hashutil.cuh:71-161,
+ * seed 0) of n HOST values of value_bytes = 1, 2, 4 or 8 bytes each. */
+int cf_hash64(uint32_t value_bytes, const void* h_values, uint64_t n, uint64_t* out);
+
+/* static getAlternateBucket(bucket, fp, numBuckets) (CuckooFilter.cuh:378-381 ->
+ * XorAltBucketPolicy::getAlternateBucket, bucket_policies.cuh:72-74) for n HOST
+ * (bucket, tag) pairs: out[i] = buckets[i] ^ (xxHash64(tag as TagType) & (num_buckets - 1)). */
+int cf_alt_buckets(const cf_config* cfg, uint64_t num_buckets, const uint64_t* buckets, const uint32_t* tags,
+                   uint64_t n, uint64_t* out);
+
 /* Lookups of this batch whose tag is in the primary bucket (one probe); the
  * rest take two probes.  Diagnostic for sector accounting. */
 int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* primary_hits, void* stream);

@@ -63,6 +63,32 @@ def test_host_hashing_matches_reference_golden(cfb, golden, kb):
     assert checked >= 3
 
 
+def test_hash64_and_alt_buckets_match_reference_golden(cfb, golden):
+    """cf_hash64 (static hash64) and cf_alt_buckets (static getAlternateBucket)
+    against the reference's own xxhash64 outputs and candidate pairs."""
+    L = cfb.library()
+    i = 0
+    while f"c{i}_meta" in golden:
+        kb, bits, bs, cap, nb = (int(x) for x in golden[f"c{i}_meta"])
+        keys = np.ascontiguousarray(golden[f"c{i}_keys"])
+        h = np.empty(len(keys), np.uint64)
+        assert L.cf_hash64(kb, keys.ctypes.data, len(keys), h.ctypes.data) == 0
+        assert np.array_equal(h, golden[f"c{i}_hash"]), i
+        cfg = _cfg(cfb, T="uint64" if kb == 8 else "uint32", bitsPerTag=bits, bucketSize=bs)
+        i1 = np.ascontiguousarray(golden[f"c{i}_i1"])
+        fp = np.ascontiguousarray(golden[f"c{i}_fp"])
+        out = np.empty(len(keys), np.uint64)
+        assert L.cf_alt_buckets(C.byref(cfg), nb, i1.ctypes.data, fp.ctypes.data, len(keys), out.ctypes.data) == 0
+        assert np.array_equal(out, golden[f"c{i}_i2"]), i
+        i += 1
+    for bits in (8, 16, 32):
+        tags = np.ascontiguousarray(golden[f"tag{bits}"].astype({8: np.uint8, 16: np.uint16, 32: np.uint32}[bits]))
+        h = np.empty(len(tags), np.uint64)
+        assert L.cf_hash64(bits // 8, tags.ctypes.data, len(tags), h.ctypes.data) == 0
+        assert np.array_equal(h, golden[f"taghash{bits}"]), bits
+    assert L.cf_hash64(3, None, 0, None) == -1
+
+
 def test_num_buckets_matches_reference(cfb, golden):
     for cap, bs, nb in golden["num_buckets"]:
         assert cfb.CuckooFilter.calculateNumBuckets(int(cap), int(bs)) == int(nb)
