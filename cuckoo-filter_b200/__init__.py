@@ -46,7 +46,14 @@ OPT_WORKSPACE_LIMIT = 1
 OPT_SEGMENTED_MIN_KEYS = 2
 OPT_WORKSPACE_BYTES = 3
 OPT_ROUND2_SEGMENTED_MIN_KEYS = 4
+OPT_REGION_MIN_KEYS = 5
+OPT_STAGING = 6
+OPT_REGION_BYTES = 7
+OPT_REGION_COUNT = 8
 NEVER = (1 << 64) - 1
+
+# cf_staging values (OPT_STAGING)
+STAGING_AUTO, STAGING_RANDOM, STAGING_SEGMENT, STAGING_REGION = 0, 1, 2, 3
 
 
 class EvictionPolicy(enum.IntEnum):

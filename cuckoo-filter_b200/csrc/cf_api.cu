@@ -41,6 +41,11 @@ struct cf_filter {
     uint64_t seg_min_keys;  // CF_OPT_SEGMENTED_MIN_KEYS (0 = automatic)
     uint64_t round2_min;    // CF_OPT_ROUND2_SEGMENTED_MIN_KEYS (0 = automatic)
     unsigned long long* h_cnt;
+    // region-staged path
+    RegionGeom rgeom;
+    uint64_t rg_min_keys;   // CF_OPT_REGION_MIN_KEYS (0 = automatic)
+    uint32_t staging;       // CF_OPT_STAGING (cf_staging)
+    uint64_t rg_bytes;      // CF_OPT_REGION_BYTES (0 = kRgRegionBytes)
 };
 
 namespace {
@@ -182,6 +187,14 @@ void init_geometry(cf_filter* f) {
     f->geom.passes = seg_bits == 0 ? 1 : (seg_bits + kRadixBits - 1) / kRadixBits;
     // (bucket << bits) | tag must fit in 64 bits for every bucket index
     f->seg_ok = ilog2(f->num_buckets) + static_cast<int>(f->cfg.bits_per_tag) <= 64;
+    // regions of ~kRgRegionBytes (or CF_OPT_REGION_BYTES), at most kRgMaxRegions of them
+    const int nb_log2 = ilog2(f->num_buckets);
+    const uint64_t rbytes = f->rg_bytes ? f->rg_bytes : kRgRegionBytes;
+    int rl = rbytes > bb ? ilog2(rbytes / bb) : 0;
+    if (rl < nb_log2 - 8) rl = nb_log2 - 8;
+    if (rl > nb_log2) rl = nb_log2;
+    f->rgeom.rl = rl;
+    f->rgeom.nreg = static_cast<uint32_t>(f->num_buckets >> rl);
 }
 
 // Bytes of workspace for a chunk of `cap` keys: two entry buffers (8 B per
@@ -200,7 +213,9 @@ int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     CF_CUDA(rs_scatter_grid<0>(f->sms, &rs_grid[0]), "radix launch setup");
     CF_CUDA(rs_scatter_grid<1>(f->sms, &rs_grid[1]), "radix launch setup");
     CF_CUDA(rs_scatter_grid<2>(f->sms, &rs_grid[2]), "radix launch setup");
-    const int grid = std::max(rs_grid[0], std::max(rs_grid[1], rs_grid[2]));
+    const int rg_grid = f->sms * 4;
+    const int grid = std::max(std::max(rs_grid[0], std::max(rs_grid[1], rs_grid[2])),
+                              (rg_grid * static_cast<int>(kRgMaxRegions) + kRadix - 1) / kRadix);
     const uint64_t fixed = ws_need(f, 0, grid, payload) + 4096;
     uint64_t cap = n;
     if (f->ws_limit > fixed) {
@@ -245,6 +260,7 @@ int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     w->h_cnt = f->h_cnt;
     w->cap = cap;
     for (int i = 0; i < 3; ++i) w->rs_grid[i] = rs_grid[i];
+    w->rg_grid = rg_grid;
     w->sms = f->sms;
     return CF_OK;
 }
@@ -282,6 +298,51 @@ int run_segmented(cf_filter* f, int op, const void* keys, uint64_t n, uint8_t* o
                 "segment-staged batch");
     }
     return CF_OK;
+}
+
+// Region-staged path (cf_region.cuh): keys from which it beats random probes.
+// A random probe costs one DRAM transaction (~38 G/s on B200); the region path
+// streams ~30 bytes per key plus the table once (lookups) or about twice
+// (inserts and deletes), at close to HBM bandwidth.
+uint64_t region_threshold(const cf_filter* f, int op) {
+    if (f->rg_min_keys) return f->rg_min_keys;
+    (void)op;
+    return UINT64_MAX;  // automatic choice: not yet (measured slower than the other paths)
+}
+
+int run_region(cf_filter* f, int op, const void* keys, uint64_t n, uint8_t* out, void* stream) {
+    if (n == 0) return CF_OK;
+    SegWork w{};
+    if (int st = ensure_workspace(f, n, op == SEG_CONTAINS || out != nullptr, &w)) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint64_t kb = f->cfg.key_bytes;
+    // lookups stage two entries per key and entry offsets are 32-bit
+    const uint64_t cap = op == SEG_CONTAINS && w.cap > (1ull << 30) ? (1ull << 30) : w.cap;
+    for (uint64_t c0 = 0; c0 < n; c0 += cap) {
+        const uint64_t m = n - c0 < cap ? n - c0 : cap;
+        CF_CUDA(f->ops->rg_chunk(dev(f), f->rgeom, w, op, static_cast<const uint8_t*>(keys) + c0 * kb, m,
+                                 out ? out + c0 : nullptr, s, f->cfg.eviction_policy == CF_EVICT_BFS ? 1u : 0u,
+                                 f->cfg.max_evictions),
+                "region-staged batch");
+    }
+    return CF_OK;
+}
+
+// Execution path of a batch: random probes, segment-staged or region-staged.
+enum Path { PATH_RANDOM, PATH_SEGMENT, PATH_REGION };
+
+Path choose_path(const cf_filter* f, int op, uint64_t n, bool sorted_insert) {
+    if (!f->seg_ok) return PATH_RANDOM;
+    switch (f->staging) {
+        case CF_STAGING_RANDOM: return sorted_insert ? PATH_SEGMENT : PATH_RANDOM;
+        case CF_STAGING_SEGMENT: return PATH_SEGMENT;
+        case CF_STAGING_REGION: return PATH_REGION;
+        default: break;
+    }
+    if (n >= region_threshold(f, op)) return PATH_REGION;
+    if (sorted_insert) return PATH_SEGMENT;
+    if (op != SEG_INSERT && n >= segmented_threshold(f, op)) return PATH_SEGMENT;
+    return PATH_RANDOM;
 }
 
 int do_insert(cf_filter* f, const void* keys, uint64_t n, uint8_t* out, void* stream) {
@@ -413,16 +474,24 @@ int cf_get_info(const cf_filter* f, cf_info* out) {
     return CF_OK;
 }
 
+int insert_any(cf_filter* f, const void* keys, uint64_t n, uint8_t* out, void* stream, bool sorted) {
+    switch (choose_path(f, SEG_INSERT, n, sorted)) {
+        case PATH_REGION: return run_region(f, SEG_INSERT, keys, n, out, stream);
+        case PATH_SEGMENT: return run_segmented(f, SEG_INSERT, keys, n, out, stream);
+        default: return do_insert(f, keys, n, out, stream);
+    }
+}
+
 int cf_insert_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
     if (int s = check_batch(f, d_keys, n)) return s;
     DeviceGuard g(f->device);
-    return do_insert(f, d_keys, n, d_out, stream);
+    return insert_any(f, d_keys, n, d_out, stream, false);
 }
 
 int cf_insert(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream, uint64_t* occupied_out) {
     if (int s = check_batch(f, d_keys, n)) return s;
     DeviceGuard g(f->device);
-    if (int s = do_insert(f, d_keys, n, d_out, stream)) return s;
+    if (int s = insert_any(f, d_keys, n, d_out, stream, false)) return s;
     return finish(f, stream, occupied_out);
 }
 
@@ -430,12 +499,8 @@ int cf_insert_sorted(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_ou
                      uint64_t* occupied_out) {
     if (int s = check_batch(f, d_keys, n)) return s;
     DeviceGuard g(f->device);
-    if (f->seg_ok) {
-        if (int s = run_segmented(f, SEG_INSERT, d_keys, n, d_out, stream)) return s;
-    } else {
-        // (bucket << bits) | tag does not fit 64 bits: the plain path
-        if (int s = do_insert(f, d_keys, n, d_out, stream)) return s;
-    }
+    // (bucket << bits) | tag must fit 64 bits for the staged paths; else the plain path
+    if (int s = insert_any(f, d_keys, n, d_out, stream, true)) return s;
     return finish(f, stream, occupied_out);
 }
 
@@ -443,7 +508,11 @@ int cf_contains_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_o
     if (int s = check_batch(f, d_keys, n)) return s;
     if (n && !d_out) return fail(CF_ERR_INVALID, "d_out is NULL with n > 0");
     DeviceGuard g(f->device);
-    if (f->seg_ok && n >= segmented_threshold(f, SEG_CONTAINS)) return run_segmented(f, SEG_CONTAINS, d_keys, n, d_out, stream);
+    switch (choose_path(f, SEG_CONTAINS, n, false)) {
+        case PATH_REGION: return run_region(f, SEG_CONTAINS, d_keys, n, d_out, stream);
+        case PATH_SEGMENT: return run_segmented(f, SEG_CONTAINS, d_keys, n, d_out, stream);
+        default: break;
+    }
     CF_CUDA(f->ops->contains(dev(f), d_keys, n, d_out, launch(f, KID_CONTAINS, stream)), "contains launch");
     return CF_OK;
 }
@@ -458,7 +527,11 @@ int cf_contains(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, vo
 int cf_delete_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
     if (int s = check_batch(f, d_keys, n)) return s;
     DeviceGuard g(f->device);
-    if (f->seg_ok && n >= segmented_threshold(f, SEG_DELETE)) return run_segmented(f, SEG_DELETE, d_keys, n, d_out, stream);
+    switch (choose_path(f, SEG_DELETE, n, false)) {
+        case PATH_REGION: return run_region(f, SEG_DELETE, d_keys, n, d_out, stream);
+        case PATH_SEGMENT: return run_segmented(f, SEG_DELETE, d_keys, n, d_out, stream);
+        default: break;
+    }
     CF_CUDA(f->ops->remove(dev(f), d_keys, n, d_out, launch(f, KID_DELETE, stream)), "delete launch");
     return CF_OK;
 }
@@ -564,6 +637,19 @@ int cf_set_option(cf_filter* f, int option, uint64_t value) {
         case CF_OPT_ROUND2_SEGMENTED_MIN_KEYS:
             f->round2_min = value;
             return CF_OK;
+        case CF_OPT_REGION_MIN_KEYS:
+            f->rg_min_keys = value;
+            return CF_OK;
+        case CF_OPT_STAGING:
+            if (value > CF_STAGING_REGION) return fail(CF_ERR_INVALID, "unknown staging mode %llu",
+                                                       static_cast<unsigned long long>(value));
+            f->staging = static_cast<uint32_t>(value);
+            return CF_OK;
+        case CF_OPT_REGION_BYTES:
+            if (value & (value - 1)) return fail(CF_ERR_INVALID, "region bytes must be 0 or a power of two");
+            f->rg_bytes = value;
+            init_geometry(f);
+            return CF_OK;
         default:
             return fail(CF_ERR_INVALID, "unknown option %d", option);
     }
@@ -577,6 +663,10 @@ int cf_get_option(cf_filter* f, int option, uint64_t* value) {
         case CF_OPT_SEGMENTED_MIN_KEYS: *value = f->seg_min_keys; return CF_OK;
         case CF_OPT_WORKSPACE_BYTES: *value = f->ws_bytes; return CF_OK;
         case CF_OPT_ROUND2_SEGMENTED_MIN_KEYS: *value = f->round2_min; return CF_OK;
+        case CF_OPT_REGION_MIN_KEYS: *value = f->rg_min_keys; return CF_OK;
+        case CF_OPT_STAGING: *value = f->staging; return CF_OK;
+        case CF_OPT_REGION_BYTES: *value = f->rg_bytes ? f->rg_bytes : kRgRegionBytes; return CF_OK;
+        case CF_OPT_REGION_COUNT: *value = f->rgeom.nreg; return CF_OK;
         default: return fail(CF_ERR_INVALID, "unknown option %d", option);
     }
 }

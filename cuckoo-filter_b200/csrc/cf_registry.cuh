@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "cf_kernels.cuh"
+#include "cf_region.cuh"
 #include "cf_segmented.cuh"
 
 namespace cfb {
@@ -37,6 +38,13 @@ struct SegWork {
     int rs_grid[3];  // radix CTAs per payload mode (one wave of that scatter kernel)
     int sms;       // streaming multiprocessors
     uint64_t round2_segmented_min;  // list length from which round 2 is segment-staged
+    int rg_grid;   // CTAs of the region partition kernels (hist entries: kRgMaxRegions * rg_grid)
+};
+
+// Geometry of the region-staged path: region = bucket >> rl, nreg regions.
+struct RegionGeom {
+    int rl;
+    uint32_t nreg;
 };
 
 // Keys per thread of each batch kernel.
@@ -65,6 +73,8 @@ struct OpsTable {
     cudaError_t (*occupancy)(int kid, int block, int* blocks_per_sm);
     cudaError_t (*seg_chunk)(const DevTable&, const SegGeom&, const SegWork&, int op, const void* keys, uint64_t m,
                              uint8_t* out, cudaStream_t, uint32_t policy_bfs, uint32_t max_ev);
+    cudaError_t (*rg_chunk)(const DevTable&, const RegionGeom&, const SegWork&, int op, const void* keys, uint64_t m,
+                            uint8_t* out, cudaStream_t, uint32_t policy_bfs, uint32_t max_ev);
 };
 
 inline bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
@@ -328,6 +338,87 @@ struct Launchers {
         }
     }
 
+    // One region partition pass: histogram, scan, scatter of `m` items
+    // (keys, or ent/pay[from] with the count on the device) into ent/pay[dst].
+    template <int MODE>
+    static void rg_split(const DevTable& t, const RegionGeom& g, const SegWork& w, const void* src,
+                         const uint32_t* src_pay, uint64_t m, const unsigned long long* m_dev, bool payload,
+                         uint64_t* dst, uint32_t* dst_pay, cudaStream_t s) {
+        const int grid = w.rg_grid;
+        k_rg_hist<C, MODE><<<grid, kRgThreads, 0, s>>>(src, t.nb_mask, m, m_dev, g.rl, g.nreg, w.hist);
+        k_scan_u32<<<1, 1024, 0, s>>>(w.hist, g.nreg * static_cast<uint32_t>(grid));
+        if (payload)
+            k_rg_scatter<C, MODE, true><<<grid, kRgThreads, 0, s>>>(src, src_pay, t.nb_mask, m, m_dev, g.rl, g.nreg,
+                                                                    w.hist, dst, dst_pay);
+        else
+            k_rg_scatter<C, MODE, false><<<grid, kRgThreads, 0, s>>>(src, nullptr, t.nb_mask, m, m_dev, g.rl, g.nreg,
+                                                                     w.hist, dst, nullptr);
+    }
+
+    template <int OP>
+    static void rg_probe(const DevTable& t, const SegWork& w, const uint64_t* ent, const uint32_t* pay, uint64_t m,
+                         const unsigned long long* m_dev, int round, uint64_t* next, uint32_t* next_pay,
+                         unsigned long long* next_count, uint32_t* bitmap, cudaStream_t s) {
+        static const int bps = blocks_per_sm(k_rg_probe<C, OP>, kRgThreads, 0);
+        k_rg_probe<C, OP><<<w.sms * bps, kRgThreads, 0, s>>>(t, ent, pay, m, m_dev, round, next, next_pay, next_count,
+                                                            bitmap);
+    }
+
+    // A chunk of m keys through the region-staged path.  Lookups: one pass
+    // with both buckets of every key.  Deletes and inserts: primary buckets,
+    // then the misses by alternate bucket, then (insert) eviction.
+    // ent/pay[0] and ent/pay[1] are adjacent buffers of w.cap entries each, so
+    // a lookup's 2m entries fit from ent/pay[0] on.
+    template <int OP>
+    static cudaError_t rg_chunk_op(const DevTable& t, const RegionGeom& g, const SegWork& w, const void* keys,
+                                   uint64_t m, uint8_t* out, cudaStream_t s, uint32_t policy_bfs, uint32_t max_ev) {
+        const bool payload = OP == SEG_CONTAINS || out != nullptr;
+        uint32_t* bm = payload ? w.bitmap : nullptr;
+        cudaError_t e = cudaMemsetAsync(w.cnt, 0, 4 * sizeof(unsigned long long), s);
+        if (e == cudaSuccess && payload) e = cudaMemsetAsync(w.bitmap, 0, (m + 31) / 32 * 4, s);
+        if (e != cudaSuccess) return e;
+        if constexpr (OP == SEG_CONTAINS) {
+            rg_split<RG_KEYS_DUAL>(t, g, w, keys, nullptr, m, nullptr, true, w.ent[0], w.pay[0], s);
+            rg_probe<OP>(t, w, w.ent[0], w.pay[0], 2 * m, nullptr, 1, nullptr, nullptr, nullptr, bm, s);
+        } else {
+            uint32_t* p0 = payload ? w.pay[0] : nullptr;
+            uint32_t* p1 = payload ? w.pay[1] : nullptr;
+            rg_split<RG_KEYS>(t, g, w, keys, nullptr, m, nullptr, payload, w.ent[0], p0, s);
+            rg_probe<OP>(t, w, w.ent[0], p0, m, nullptr, 1, w.ent[1], p1, &w.cnt[0], bm, s);
+            rg_split<RG_ENT>(t, g, w, w.ent[1], p1, 0, &w.cnt[0], payload, w.ent[0], p0, s);
+            rg_probe<OP>(t, w, w.ent[0], p0, 0, &w.cnt[0], 2, OP == SEG_INSERT ? w.ent[1] : nullptr,
+                         OP == SEG_INSERT ? p1 : nullptr, &w.cnt[1], bm, s);
+            if constexpr (OP == SEG_INSERT) {
+                // keys whose two buckets are full: ent/pay[1], count cnt[1]
+                static const int bfs_bps = blocks_per_sm(k_evict_bfs_steps<C>, 256, 0);
+                static const int list_bps = blocks_per_sm(k_evict_list<C>, 256, 0);
+                if (policy_bfs) {
+                    k_evict_bfs_steps<C><<<w.sms * bfs_bps, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], bm, w.ent[0], p0,
+                                                                       &w.cnt[2]);
+                    k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[0], p0, &w.cnt[2], 0u, max_ev, bm, 1u);
+                } else {
+                    k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], 0u, max_ev, bm, 0u);
+                }
+            }
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess && payload) {
+            const int xgrid = static_cast<int>(((m + 31) / 32 + 255) / 256 < 8192 ? ((m + 31) / 32 + 255) / 256 : 8192);
+            k_bitmap_expand<<<xgrid, 256, 0, s>>>(w.bitmap, m, out);
+            e = cudaGetLastError();
+        }
+        return e;
+    }
+
+    static cudaError_t rg_chunk(const DevTable& t, const RegionGeom& g, const SegWork& w, int op, const void* keys,
+                                uint64_t m, uint8_t* out, cudaStream_t s, uint32_t policy_bfs, uint32_t max_ev) {
+        switch (op) {
+            case SEG_INSERT: return rg_chunk_op<SEG_INSERT>(t, g, w, keys, m, out, s, policy_bfs, max_ev);
+            case SEG_CONTAINS: return rg_chunk_op<SEG_CONTAINS>(t, g, w, keys, m, out, s, policy_bfs, max_ev);
+            default: return rg_chunk_op<SEG_DELETE>(t, g, w, keys, m, out, s, policy_bfs, max_ev);
+        }
+    }
+
     static OpsTable table() {
         OpsTable o{};
         o.key_bytes = C::key_bytes;
@@ -345,6 +436,7 @@ struct Launchers {
         o.probe = probe;
         o.occupancy = occupancy;
         o.seg_chunk = seg_chunk;
+        o.rg_chunk = rg_chunk;
         return o;
     }
 };

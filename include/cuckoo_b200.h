@@ -186,8 +186,30 @@ typedef enum cf_option {
     /* Inside a segment-staged batch: number of keys that missed their primary
      * bucket from which the alternate-bucket round is segment-staged too
      * (otherwise those keys are probed at random).  0 = automatic, as above. */
-    CF_OPT_ROUND2_SEGMENTED_MIN_KEYS = 4
+    CF_OPT_ROUND2_SEGMENTED_MIN_KEYS = 4,
+    /* Batch size from which every operation is region-staged: the batch is
+     * partitioned by ~16 MiB table region in one pass and applied region by
+     * region, so probes hit L2.  0 = automatic (table bytes / 128 keys for
+     * lookups, / 64 for inserts and deletes); UINT64_MAX = never. */
+    CF_OPT_REGION_MIN_KEYS = 5,
+    /* Force one execution path for every batch (cf_staging); CF_STAGING_AUTO
+     * (default) picks by batch size as described above. */
+    CF_OPT_STAGING = 6,
+    /* Table bytes per region of the region-staged path: a power of two,
+     * 0 = default (16 MiB).  The table is cut into at most 256 regions, so
+     * tables above 4 GiB get larger regions. */
+    CF_OPT_REGION_BYTES = 7,
+    /* Read-only: number of regions of the region-staged path. */
+    CF_OPT_REGION_COUNT = 8
 } cf_option;
+
+/* Execution paths (CF_OPT_STAGING).  All give the same per-key results. */
+typedef enum cf_staging {
+    CF_STAGING_AUTO = 0,
+    CF_STAGING_RANDOM = 1,  /* one probe per bucket at random (insertManySorted: segment-staged) */
+    CF_STAGING_SEGMENT = 2, /* sort by 64 KiB segment, stage segments in shared memory */
+    CF_STAGING_REGION = 3   /* partition by ~16 MiB region, apply in region order through L2 */
+} cf_staging;
 
 int cf_set_option(cf_filter* f, int option, uint64_t value);
 int cf_get_option(cf_filter* f, int option, uint64_t* value);

@@ -39,10 +39,16 @@ def host_u8(t) -> np.ndarray:
     return t.to(torch.uint8).cpu().numpy()
 
 
-def make(cfb, orc, key_bytes=8, bits=16, bs=16, policy=1, max_ev=500, capacity=1 << 12):
+STAGING = {"auto": 0, "random": 1, "segment": 2, "region": 3}
+
+
+def make(cfb, orc, key_bytes=8, bits=16, bs=16, policy=1, max_ev=500, capacity=1 << 12, staging="auto"):
+    """A filter and the oracle of the same geometry; `staging` forces an
+    execution path (CF_OPT_STAGING) for every batch of the filter."""
     cfg = cfb.CuckooConfig(T="uint64" if key_bytes == 8 else "uint32", bitsPerTag=bits, bucketSize=bs,
                            maxEvictions=max_ev, evictionPolicy=cfb.EvictionPolicy(policy))
     f = cfb.CuckooFilter(cfg, capacity)
+    f.setOption(cfb.OPT_STAGING, STAGING[staging])
     o = orc.OracleFilter(key_bytes=key_bytes, bits=bits, bucket_size=bs, policy=policy, max_evictions=max_ev,
                          capacity=capacity, mode=orc.MODE_CONSERVING)
     assert f.getNumBuckets() == o.nb
@@ -199,10 +205,11 @@ def _stored_invariants(f, o, orc, stored_keys):
 BULK_CASES = [(8, 16, 16, 0), (8, 16, 16, 1), (8, 8, 16, 0), (8, 32, 8, 1), (8, 32, 8, 0), (4, 16, 16, 1)]
 
 
+@pytest.mark.parametrize("staging", ["random", "region"])
 @pytest.mark.parametrize("kb,bits,bs,policy", BULK_CASES)
-def test_bulk_insert_invariants(cfb, orc, kb, bits, bs, policy):
+def test_bulk_insert_invariants(cfb, orc, kb, bits, bs, policy, staging):
     """Small config: 2^20 slots filled to 0.95 (996 147 keys, splitmix64 seed 1)."""
-    f, o = make(cfb, orc, kb, bits, bs, policy, 500, 1 << 20)
+    f, o = make(cfb, orc, kb, bits, bs, policy, 500, 1 << 20, staging)
     keys = orc.splitmix64(1, int(0.95 * f.capacity()))
     if kb == 4:
         keys = np.unique(keys.astype(np.uint32))
@@ -266,10 +273,11 @@ def test_sequential_delete_bit_exact(cfb, orc, kb, bits, bs):
     assert f.occupiedSlots() == o.occupied()
 
 
+@pytest.mark.parametrize("staging", ["random", "region"])
 @pytest.mark.parametrize("kb,bits,bs,policy", [(8, 16, 16, 0), (8, 32, 8, 1), (4, 16, 16, 1)])
-def test_bulk_delete(cfb, orc, kb, bits, bs, policy):
+def test_bulk_delete(cfb, orc, kb, bits, bs, policy, staging):
     """Insert at 0.95, delete the first half, re-query (the reference's example flow, src/main.cu:128-175)."""
-    f, o = make(cfb, orc, kb, bits, bs, policy, 500, 1 << 20)
+    f, o = make(cfb, orc, kb, bits, bs, policy, 500, 1 << 20, staging)
     keys = orc.splitmix64(1, int(0.95 * f.capacity()))
     if kb == 4:
         keys = np.unique(keys.astype(np.uint32))
@@ -317,8 +325,9 @@ def test_duplicate_keys_overflow_without_loss(cfb, orc):
 
 
 @pytest.mark.parametrize("n", [0, 1, 2, 3, 5, 31, 33, 255, 257, 1023, 4097, 100_003])
-def test_ragged_sizes(cfb, orc, n):
-    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 18)
+@pytest.mark.parametrize("staging", ["random", "segment", "region"])
+def test_ragged_sizes(cfb, orc, n, staging):
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 18, staging)
     keys = orc.splitmix64(9, n)
     d = dev(keys) if n else torch.empty(0, dtype=torch.int64, device="cuda")
     out = torch.zeros(n, dtype=torch.bool, device="cuda")
@@ -330,9 +339,10 @@ def test_ragged_sizes(cfb, orc, n):
 
 
 @pytest.mark.parametrize("offset", [1, 2, 3, 5])
-def test_unaligned_pointers(cfb, orc, offset):
+@pytest.mark.parametrize("staging", ["random", "region"])
+def test_unaligned_pointers(cfb, orc, offset, staging):
     """Key and output pointers that are not vector-aligned take the scalar path."""
-    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 16)
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 16, staging)
     keys = orc.splitmix64(13, 40_000)
     buf = dev(np.concatenate([np.zeros(offset, np.uint64), keys]))
     d = buf[offset:]
