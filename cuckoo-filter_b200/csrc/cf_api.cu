@@ -7,6 +7,7 @@
 // `this` pointer.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -203,7 +204,8 @@ uint64_t ws_need(const cf_filter* f, uint64_t cap, int grid, bool payload) {
     const uint64_t hist = static_cast<uint64_t>(kRadix) * grid * 4;
     const uint64_t start = (f->geom.nseg + 1) * 4;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-    const uint64_t per_key = payload ? al(cap * 4) * 2 + al((cap + 31) / 32 * 4) : 0;
+    // result bitmap: two bits per key (a region-staged lookup keeps one hit bit per staged entry)
+    const uint64_t per_key = payload ? al(cap * 4) * 2 + al((2 * cap + 31) / 32 * 4) : 0;
     return al(cap * 8) * 2 + per_key + al(hist) + al(start) + al(64);
 }
 
@@ -316,8 +318,13 @@ int run_region(cf_filter* f, int op, const void* keys, uint64_t n, uint8_t* out,
     if (int st = ensure_workspace(f, n, op == SEG_CONTAINS || out != nullptr, &w)) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint64_t kb = f->cfg.key_bytes;
-    // lookups stage two entries per key and entry offsets are 32-bit
-    const uint64_t cap = op == SEG_CONTAINS && w.cap > (1ull << 30) ? (1ull << 30) : w.cap;
+    // lookups stage two entries per key (32-bit entry offsets) and gather each
+    // partition chunk's results in shared memory: at most 2^29 keys per chunk
+    uint64_t cap = w.cap;
+    if (op == SEG_CONTAINS) {
+        const uint64_t lim = std::min<uint64_t>(1ull << 29, static_cast<uint64_t>(w.rg_grid) * 1000000ull);
+        if (cap > lim) cap = lim;
+    }
     for (uint64_t c0 = 0; c0 < n; c0 += cap) {
         const uint64_t m = n - c0 < cap ? n - c0 : cap;
         CF_CUDA(f->ops->rg_chunk(dev(f), f->rgeom, w, op, static_cast<const uint8_t*>(keys) + c0 * kb, m,

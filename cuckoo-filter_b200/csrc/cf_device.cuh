@@ -185,6 +185,25 @@ __device__ __forceinline__ void load_nc(const void* p, uint64_t* c) {
     }
 }
 
+// As load_nc, but the loads stay in program order relative to each other, so a
+// run of them is issued back to back before any result is used (the compiler
+// may otherwise sink each load next to its use and serialize them).
+template <int BYTES>
+__device__ __forceinline__ void load_nc_issue(const void* p, uint64_t* c) {
+    if constexpr (BYTES == 8) {
+        asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(c[0]) : "l"(p));
+    } else if constexpr (BYTES == 16) {
+        asm volatile("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];" : "=l"(c[0]), "=l"(c[1]) : "l"(p));
+    } else {
+#pragma unroll
+        for (int i = 0; i < BYTES / 32; ++i) {
+            asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                         : "=l"(c[4 * i]), "=l"(c[4 * i + 1]), "=l"(c[4 * i + 2]), "=l"(c[4 * i + 3])
+                         : "l"(static_cast<const char*>(p) + 32 * i));
+        }
+    }
+}
+
 // Bucket load for read-modify-write paths: relaxed at GPU scope so the values
 // are at least as new as L2; they only seed compare-and-swap expectations.
 template <int BYTES>
@@ -239,6 +258,23 @@ __device__ __forceinline__ void ld_stream_v4u32(const uint32_t* p, uint32_t& a, 
     asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
                  : "l"(p));
+}
+
+// Streaming loads that L2 may evict first (data read once).
+__device__ __forceinline__ uint64_t ld_once_u64(const uint64_t* p) {
+    return static_cast<uint64_t>(__ldcs(reinterpret_cast<const unsigned long long*>(p)));
+}
+__device__ __forceinline__ uint32_t ld_once_u32(const uint32_t* p) { return __ldcs(p); }
+
+// L2 policy that keeps lines resident ahead of normal and streaming data.
+__device__ __forceinline__ uint64_t l2_policy_keep() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// Fire-and-forget bitwise OR into global memory under an L2 cache policy.
+__device__ __forceinline__ void red_or_policy(uint32_t* p, uint32_t v, uint64_t pol) {
+    asm volatile("red.relaxed.gpu.global.or.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
 }
 
 // ------------------------------------------- bulk copies (TMA) and mbarriers

@@ -57,12 +57,14 @@ __device__ __forceinline__ uint64_t rg_chunk(uint64_t m) {
     return (per + T - 1) / T * T;
 }
 
+// Keys and staged entries are read once: streaming loads, evicted from L2
+// first, so the table region and the result bitmap stay resident.
 template <class C>
 __device__ __forceinline__ uint64_t rg_load_key(const void* keys, uint64_t i) {
     if constexpr (C::key_bytes == 8)
-        return ld_stream_u64(static_cast<const uint64_t*>(keys) + i);
+        return ld_once_u64(static_cast<const uint64_t*>(keys) + i);
     else
-        return ld_stream_u32(static_cast<const uint32_t*>(keys) + i);
+        return ld_once_u32(static_cast<const uint32_t*>(keys) + i);
 }
 
 // Per-CTA region histogram of its contiguous share: hist[region * grid + cta].
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_hist(const void* src, uint64_
             x[j] = 0;
             if (i < hi) {
                 if constexpr (MODE == RG_ENT)
-                    x[j] = ld_stream_u64(static_cast<const uint64_t*>(src) + i);
+                    x[j] = ld_once_u64(static_cast<const uint64_t*>(src) + i);
                 else
                     x[j] = rg_load_key<C>(src, i);
             }
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_hist(const void* src, uint64_
 // shared-memory atomic per entry (order within a region is not kept), staged
 // in region order and written out as contiguous runs.  PAY: write payloads.
 template <class C, int MODE, bool PAY>
-__global__ void __launch_bounds__(kRgThreads) k_rg_scatter(const void* src, const uint32_t* __restrict__ src_pay,
+__global__ void __launch_bounds__(kRgThreads, 3) k_rg_scatter(const void* src, const uint32_t* __restrict__ src_pay,
                                                            uint64_t nb_mask, uint64_t n,
                                                            const unsigned long long* n_dev, int rl, uint32_t nreg,
                                                            const uint32_t* __restrict__ offs, uint64_t* __restrict__ dst,
@@ -141,49 +143,56 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_scatter(const void* src, cons
     constexpr int T = rg_items_per_tile<MODE>();
     constexpr int IPT = T / kRgThreads;                  // items per thread
     constexpr int EPI = MODE == RG_KEYS_DUAL ? 2 : 1;   // entries per item
-    for (uint64_t tb = lo; tb < hi; tb += T) {
-        const uint32_t count_items = static_cast<uint32_t>(hi - tb < static_cast<uint64_t>(T) ? hi - tb : T);
-        uint64_t e[IPT * EPI];
-        uint32_t p[IPT * EPI], rank[IPT * EPI], dig[IPT * EPI];
-        uint64_t x[IPT];
-        uint32_t xp[IPT];
+    // the next tile's items are loaded while the current tile is ranked and
+    // written, so their DRAM latency overlaps this tile's shared-memory work
+    uint64_t xn[IPT];
+    uint32_t xpn[IPT];
+    auto fetch = [&](uint64_t tb) {
+        const uint32_t cnt_items = static_cast<uint32_t>(hi - tb < static_cast<uint64_t>(T) ? hi - tb : T);
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
             const uint32_t q = j * kRgThreads + tid;
-            x[j] = 0;
-            xp[j] = 0;
-            if (q < count_items) {
+            xn[j] = 0;
+            xpn[j] = 0;
+            if (q < cnt_items) {
                 if constexpr (MODE == RG_ENT) {
-                    x[j] = ld_stream_u64(static_cast<const uint64_t*>(src) + tb + q);
-                    if constexpr (PAY) xp[j] = ld_stream_u32(src_pay + tb + q);
+                    xn[j] = ld_once_u64(static_cast<const uint64_t*>(src) + tb + q);
+                    if constexpr (PAY) xpn[j] = ld_once_u32(src_pay + tb + q);
                 } else {
-                    x[j] = rg_load_key<C>(src, tb + q);
-                    xp[j] = static_cast<uint32_t>(tb + q);
+                    xn[j] = rg_load_key<C>(src, tb + q);
                 }
             }
         }
+    };
+    if (lo < hi) fetch(lo);
+    for (uint64_t tb = lo; tb < hi; tb += T) {
+        const uint32_t count_items = static_cast<uint32_t>(hi - tb < static_cast<uint64_t>(T) ? hi - tb : T);
+        uint64_t e[IPT * EPI];
+        uint32_t p[IPT];            // payload per item (both entries of a key share it)
+        uint32_t rd[IPT * EPI];     // rank << 16 | region (region kRgMaxRegions = no entry)
+        uint64_t x[IPT];
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+            x[j] = xn[j];
+            p[j] = MODE == RG_ENT ? xpn[j] : static_cast<uint32_t>(tb + j * kRgThreads + tid);
+        }
+        if (tb + T < hi) fetch(tb + T);
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
             const bool v = j * kRgThreads + tid < count_items;
             if constexpr (MODE == RG_ENT) {
                 e[j] = x[j];
-                p[j] = xp[j];
             } else {
                 uint64_t i1;
                 uint32_t fp;
                 candidates<C>(x[j], nb_mask, i1, fp);
                 e[j * EPI] = pack_entry<C>(i1, fp);
-                p[j * EPI] = xp[j];
-                if constexpr (MODE == RG_KEYS_DUAL) {
-                    e[j * EPI + 1] = pack_entry<C>(alt_bucket<C>(i1, fp, nb_mask), fp);
-                    p[j * EPI + 1] = xp[j];
-                }
+                if constexpr (MODE == RG_KEYS_DUAL) e[j * EPI + 1] = pack_entry<C>(alt_bucket<C>(i1, fp, nb_mask), fp);
             }
 #pragma unroll
             for (int k = 0; k < EPI; ++k) {
                 const uint32_t d = static_cast<uint32_t>(e[j * EPI + k] >> ebits);
-                dig[j * EPI + k] = v ? d : kRgMaxRegions;
-                rank[j * EPI + k] = v ? atomicAdd(&cnt[d], 1u) : 0u;
+                rd[j * EPI + k] = v ? (atomicAdd(&cnt[d], 1u) << 16) | d : kRgMaxRegions;
             }
         }
         __syncthreads();
@@ -204,21 +213,23 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_scatter(const void* src, cons
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < IPT * EPI; ++k) {
-            const uint32_t d = dig[k];
+            const uint32_t d = rd[k] & 0xFFFFu;
             if (d < kRgMaxRegions) {
-                const uint32_t pos = toff[d] + rank[k];
+                const uint32_t pos = toff[d] + (rd[k] >> 16);
                 st_e[pos] = e[k];
-                if constexpr (PAY) st_p[pos] = p[k];
+                if constexpr (PAY) st_p[pos] = p[k / EPI];
             }
         }
         __syncthreads();
+        // ordinary write-back stores: a region's run from this tile and the
+        // next tile's run meet in L2 and leave for DRAM as whole lines
         const uint32_t count_e = count_items * EPI;
         for (uint32_t q = tid; q < count_e; q += kRgThreads) {
             const uint64_t v = st_e[q];
             const uint32_t d = static_cast<uint32_t>(v >> ebits);
             const uint32_t g = running[d] + (q - toff[d]);
-            __stcs(reinterpret_cast<unsigned long long*>(dst) + g, v);
-            if constexpr (PAY) __stcs(dst_pay + g, st_p[q]);
+            dst[g] = v;
+            if constexpr (PAY) dst_pay[g] = st_p[q];
         }
         __syncthreads();
         running[tid] += cnt[tid];
@@ -246,6 +257,7 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_probe(DevTable t, const uint6
     const uint32_t tid = threadIdx.x, lane = tid & 31;
     const uint64_t m = item_count(n, n_dev);
     const uint64_t tile = static_cast<uint64_t>(kRgThreads) * U;
+    const uint64_t keep = l2_policy_keep();  // the result bitmap stays in L2
     uint32_t n_ok = 0;
     bool err = false;
     for (uint64_t base = blockIdx.x * tile; base < m; base += static_cast<uint64_t>(gridDim.x) * tile) {
@@ -258,8 +270,8 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_probe(DevTable t, const uint6
             ev[j] = 0;
             pv[j] = 0;
             if (k < m) {
-                ev[j] = ld_stream_u64(ent + k);
-                if (pay) pv[j] = ld_stream_u32(pay + k);
+                ev[j] = ld_once_u64(ent + k);
+                if (pay) pv[j] = ld_once_u32(pay + k);
             }
         }
 #pragma unroll
@@ -287,7 +299,7 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_probe(DevTable t, const uint6
                 ok = has_tag<C>(c[j], fp);
             else
                 ok = try_remove<C>(bw, c[j], fp, err);
-            if (ok && bitmap) atomicOr(&bitmap[pv[j] >> 5], 1u << (pv[j] & 31));
+            if (ok && bitmap) red_or_policy(&bitmap[pv[j] >> 5], 1u << (pv[j] & 31), keep);
             n_ok += ok ? 1u : 0u;
             if (!ok && next) fwd_mask |= 1u << j;
         }
@@ -331,6 +343,96 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_probe(DevTable t, const uint6
         }
     }
     if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// Lookup walk of region-partitioned entries (both buckets of every key were
+// staged, RG_KEYS_DUAL).  Like k_rg_probe, but the outcome of entry k is
+// written as bit k of `hits` (one ballot word per warp and step, in entry
+// order), so the walk's only writes are sequential; k_rg_gather turns the
+// bits into per-key results.
+template <class C>
+__global__ void __launch_bounds__(kRgThreads, 3) k_rg_lookup(DevTable t, const uint64_t* __restrict__ ent, uint64_t m,
+                                                            uint32_t* __restrict__ hits) {
+    constexpr int U = C::bucket_bytes > 32 ? 3 : C::bucket_bytes > 16 ? 6 : 8;  // bucket loads in flight per thread
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t tile = static_cast<uint64_t>(kRgThreads) * U;
+    for (uint64_t base = blockIdx.x * tile; base < m; base += static_cast<uint64_t>(gridDim.x) * tile) {
+        uint64_t ev[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint64_t k = base + static_cast<uint64_t>(j) * kRgThreads + threadIdx.x;
+            ev[j] = k < m ? ld_once_u64(ent + k) : 0;
+        }
+        uint64_t c[U][C::nchunks];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint64_t k = base + static_cast<uint64_t>(j) * kRgThreads + threadIdx.x;
+            if (k < m) load_nc_issue<C::bucket_bytes>(t.buckets + (ev[j] >> C::bits) * C::bucket_bytes, c[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint64_t k = base + static_cast<uint64_t>(j) * kRgThreads + threadIdx.x;
+            const bool hit = k < m && has_tag<C>(c[j], static_cast<uint32_t>(ev[j]) & C::tag_mask);
+            const uint32_t word = __ballot_sync(0xFFFFFFFFu, hit);
+            const uint64_t k0 = base + static_cast<uint64_t>(j) * kRgThreads + warp * 32;  // multiple of 32
+            if (lane == 0 && k0 < m) hits[k0 >> 5] = word;
+        }
+    }
+}
+
+// Per-key lookup results from the entry-order hit bits.  CTA c owns the keys
+// of the partition pass's chunk c (same grid and chunking as k_rg_scatter) and
+// reads, region by region, the run of entries that chunk c contributed to each
+// region: offs (the scanned histogram, [region][cta]) gives each run's start
+// and the next element its end.  The payload of an entry is its key's index;
+// hits are OR-ed into a shared-memory bitmap of the chunk (dynamic shared
+// memory: one bit per key of the chunk), then written out as bytes in order.
+static __global__ void __launch_bounds__(kRgThreads) k_rg_gather(const uint32_t* __restrict__ pay,
+                                                          const uint32_t* __restrict__ hits,
+                                                          const uint32_t* __restrict__ offs, uint32_t nreg,
+                                                          uint64_t m, uint64_t total, uint8_t* __restrict__ out) {
+    extern __shared__ uint32_t sbm[];
+    const uint64_t chunk = rg_chunk<RG_KEYS_DUAL>(m);
+    const uint64_t lo = blockIdx.x * chunk;
+    if (lo >= m) return;
+    const uint64_t hi = lo + chunk < m ? lo + chunk : m;
+    const uint32_t nwords = static_cast<uint32_t>((hi - lo + 31) / 32);
+    for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) sbm[i] = 0;
+    __syncthreads();
+    const uint64_t nflat = static_cast<uint64_t>(nreg) * gridDim.x;
+    for (uint32_t r = 0; r < nreg; ++r) {
+        const uint64_t idx = static_cast<uint64_t>(r) * gridDim.x + blockIdx.x;
+        const uint64_t s = offs[idx];
+        const uint64_t e = idx + 1 < nflat ? offs[idx + 1] : total;
+        for (uint64_t k = s + threadIdx.x; k < e; k += blockDim.x) {
+            if ((hits[k >> 5] >> (k & 31)) & 1u) {
+                const uint32_t q = static_cast<uint32_t>(pay[k] - lo);
+                atomicOr(&sbm[q >> 5], 1u << (q & 31));
+            }
+        }
+    }
+    __syncthreads();
+    const uint64_t cnt = hi - lo;
+    if ((reinterpret_cast<uintptr_t>(out + lo) & 15) == 0) {
+        // 16 results per thread and store
+        for (uint64_t q0 = static_cast<uint64_t>(threadIdx.x) * 16; q0 < cnt; q0 += static_cast<uint64_t>(blockDim.x) * 16) {
+            if (q0 + 16 <= cnt) {
+                const uint32_t bits = (sbm[q0 >> 5] >> (q0 & 31)) & 0xFFFFu;
+                uint64_t lo8 = 0, hi8 = 0;
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    lo8 |= static_cast<uint64_t>((bits >> b) & 1u) << (8 * b);
+                    hi8 |= static_cast<uint64_t>((bits >> (b + 8)) & 1u) << (8 * b);
+                }
+                *reinterpret_cast<ulonglong2*>(out + lo + q0) = make_ulonglong2(lo8, hi8);
+            } else {
+                for (uint64_t q = q0; q < cnt; ++q) out[lo + q] = static_cast<uint8_t>((sbm[q >> 5] >> (q & 31)) & 1u);
+            }
+        }
+    } else {
+        for (uint64_t q = threadIdx.x; q < cnt; q += blockDim.x)
+            out[lo + q] = static_cast<uint8_t>((sbm[q >> 5] >> (q & 31)) & 1u);
+    }
 }
 
 }  // namespace cfb

@@ -47,6 +47,9 @@ struct RegionGeom {
     uint32_t nreg;
 };
 
+// Dynamic shared memory limit of k_rg_gather (one bit per key of a chunk).
+constexpr int kRgGatherMaxSmem = 160 * 1024;
+
 // Keys per thread of each batch kernel.
 constexpr int kContainsKPT = 4;
 constexpr int kDeleteKPT = 4;
@@ -378,8 +381,19 @@ struct Launchers {
         if (e == cudaSuccess && payload) e = cudaMemsetAsync(w.bitmap, 0, (m + 31) / 32 * 4, s);
         if (e != cudaSuccess) return e;
         if constexpr (OP == SEG_CONTAINS) {
+            // both buckets of every key in one partition pass; hit bits in entry
+            // order (w.bitmap, 2m bits); per-chunk gather writes `out`
             rg_split<RG_KEYS_DUAL>(t, g, w, keys, nullptr, m, nullptr, true, w.ent[0], w.pay[0], s);
-            rg_probe<OP>(t, w, w.ent[0], w.pay[0], 2 * m, nullptr, 1, nullptr, nullptr, nullptr, bm, s);
+            static const int lk_bps = blocks_per_sm(k_rg_lookup<C>, kRgThreads, 0);
+            k_rg_lookup<C><<<w.sms * lk_bps, kRgThreads, 0, s>>>(t, w.ent[0], 2 * m, w.bitmap);
+            e = ensure_smem_attr<k_rg_gather>(kRgGatherMaxSmem);
+            if (e != cudaSuccess) return e;
+            const uint64_t per = (m + w.rg_grid - 1) / w.rg_grid;
+            const uint64_t chunk = (per + kRgTile / 2 - 1) / (kRgTile / 2) * (kRgTile / 2);
+            const int smem = static_cast<int>((chunk + 31) / 32 * 4);
+            if (smem > kRgGatherMaxSmem) return cudaErrorInvalidValue;
+            k_rg_gather<<<w.rg_grid, kRgThreads, smem, s>>>(w.pay[0], w.bitmap, w.hist, g.nreg, m, 2 * m, out);
+            return cudaGetLastError();
         } else {
             uint32_t* p0 = payload ? w.pay[0] : nullptr;
             uint32_t* p1 = payload ? w.pay[1] : nullptr;
