@@ -120,6 +120,8 @@ def library() -> C.CDLL:
         "cf_probe_count": ([vp, vp, u64, P64, vp], i32),
         "cf_hash_candidates": ([C.POINTER(_Config), u64, vp, u64, vp, vp, vp], i32),
         "cf_hash64": ([u32, vp, u64, vp], i32),
+        "cf_insert_sorted_noalloc": ([vp, vp, u64, vp, vp, P64], i32),
+        "cf_noalloc_scratch_bytes": ([], u64),
         "cf_alt_buckets": ([C.POINTER(_Config), u64, vp, vp, u64, vp], i32),
         "cf_set_option": ([vp, i32, u64], i32),
         "cf_get_option": ([vp, i32, P64], i32),

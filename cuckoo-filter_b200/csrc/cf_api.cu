@@ -756,3 +756,113 @@ int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* prima
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Sorted insert without allocation (cf_insert_sorted_noalloc).
+//
+// cf_insert_sorted grows a cudaMalloc'd workspace on demand and may free and
+// re-allocate it.  Some callers cannot allow that: a cudaMalloc or cudaFree
+// can synchronize the whole device (stalling other streams of a serving
+// process), allocation is not permitted while a stream is being captured, and
+// some hosts hand the library a device whose memory is already fully reserved
+// by another allocator.  For them the segment-staged insert runs here on a
+// fixed scratch area that is part of the library's own device image: a
+// file-scope __device__ array, present on every GPU on which this library's
+// code is loaded, until the process exits.  Nothing is allocated per call.
+
+namespace {
+
+constexpr uint64_t kNoAllocMaxKeys = CF_NOALLOC_MAX_KEYS;
+constexpr uint64_t kNoAllocMaxSegments = 1ull << 18;  // tables up to 16 GiB (64 KiB segments)
+constexpr int kNoAllocMaxGrid = 2048;                  // radix-pass CTAs
+
+constexpr uint64_t na_al(uint64_t x) { return (x + 255) & ~255ull; }
+// Layout: two entry buffers, two payload buffers, the result bitmap (two bits
+// per key, as the workspace allocator sizes it), the radix histogram, the
+// segment starts and the list counters.
+constexpr uint64_t kNaEnt = na_al(kNoAllocMaxKeys * 8);
+constexpr uint64_t kNaPay = na_al(kNoAllocMaxKeys * 4);
+constexpr uint64_t kNaBitmap = na_al((2 * kNoAllocMaxKeys + 31) / 32 * 4);
+constexpr uint64_t kNaHist = na_al(static_cast<uint64_t>(kRadix) * kNoAllocMaxGrid * 4);
+constexpr uint64_t kNaStart = na_al((kNoAllocMaxSegments + 1) * 4);
+constexpr uint64_t kNaCnt = 256;
+constexpr uint64_t kNoAllocScratchBytes = 2 * kNaEnt + 2 * kNaPay + kNaBitmap + kNaHist + kNaStart + kNaCnt;
+
+// The scratch.  In host code this name is only a handle: its device address
+// comes from cudaGetSymbolAddress, once per device (noalloc_scratch).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch on the current device (looked up on the
+// first call per device).
+int noalloc_scratch(int device, void** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(CF_ERR_UNSUPPORTED, "device ordinal %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "scratch address lookup");
+        g_noalloc_ptr[device] = p;
+    }
+    *out = g_noalloc_ptr[device];
+    return CF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t cf_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+
+int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,
+                             uint64_t* occupied_out) {
+    if (int s = check_batch(f, d_keys, n)) return s;
+    if (n > kNoAllocMaxKeys)
+        return fail(CF_ERR_INVALID, "%llu keys exceed the %llu-key limit of cf_insert_sorted_noalloc; split the batch",
+                    static_cast<unsigned long long>(n), static_cast<unsigned long long>(kNoAllocMaxKeys));
+    if (!f->seg_ok)
+        return fail(CF_ERR_UNSUPPORTED, "bucket index and tag do not fit one 64-bit entry for this table");
+    if (f->geom.nseg > kNoAllocMaxSegments)
+        return fail(CF_ERR_UNSUPPORTED, "table of %llu segments exceeds the %llu-segment limit of the fixed scratch",
+                    static_cast<unsigned long long>(f->geom.nseg), static_cast<unsigned long long>(kNoAllocMaxSegments));
+    DeviceGuard g(f->device);
+    void* base = nullptr;
+    if (int s = noalloc_scratch(f->device, &base)) return s;
+    SegWork w{};
+    CF_CUDA(rs_scatter_grid<0>(f->sms, &w.rs_grid[0]), "radix launch setup");
+    CF_CUDA(rs_scatter_grid<1>(f->sms, &w.rs_grid[1]), "radix launch setup");
+    CF_CUDA(rs_scatter_grid<2>(f->sms, &w.rs_grid[2]), "radix launch setup");
+    for (int i = 0; i < 3; ++i)
+        if (w.rs_grid[i] > kNoAllocMaxGrid) return fail(CF_ERR_UNSUPPORTED, "radix grid %d too large", w.rs_grid[i]);
+    uint8_t* p = static_cast<uint8_t*>(base);
+    w.ent[0] = reinterpret_cast<uint64_t*>(p);
+    w.ent[1] = reinterpret_cast<uint64_t*>(p + kNaEnt);
+    p += 2 * kNaEnt;
+    w.pay[0] = reinterpret_cast<uint32_t*>(p);
+    w.pay[1] = reinterpret_cast<uint32_t*>(p + kNaPay);
+    p += 2 * kNaPay;
+    w.bitmap = reinterpret_cast<uint32_t*>(p);
+    p += kNaBitmap;
+    w.hist = reinterpret_cast<uint32_t*>(p);
+    p += kNaHist;
+    w.start = reinterpret_cast<uint32_t*>(p);
+    p += kNaStart;
+    w.cnt = reinterpret_cast<unsigned long long*>(p);
+    w.h_cnt = f->h_cnt;
+    w.cap = kNoAllocMaxKeys;
+    w.sms = f->sms;
+    w.rg_grid = f->sms * 4;
+    w.round2_segmented_min = f->round2_min ? f->round2_min : auto_threshold(f, SEG_INSERT);
+    if (n) {
+        // the segment pass clears the list counters, the result bitmap and the
+        // segment starts itself; the other buffers are written before read
+        CF_CUDA(f->ops->seg_chunk(dev(f), f->geom, w, SEG_INSERT, d_keys, n, d_out, static_cast<cudaStream_t>(stream),
+                                  f->cfg.eviction_policy == CF_EVICT_BFS ? 1u : 0u, f->cfg.max_evictions),
+                "segment-staged batch");
+    }
+    return finish(f, stream, occupied_out);
+}
+
+}  // extern "C"

@@ -233,6 +233,37 @@ int cf_hash64(uint32_t value_bytes, const void* h_values, uint64_t n, uint64_t* 
 int cf_alt_buckets(const cf_config* cfg, uint64_t num_buckets, const uint64_t* buckets, const uint32_t* tags,
                    uint64_t n, uint64_t* out);
 
+/*
+ * insertManySorted for callers that cannot allocate device memory.  No
+ * counterpart in the reference (whose insertManySorted calls cudaMalloc and
+ * cudaFree inside every call, CuckooFilter.cuh:475-508).
+ *
+ * cf_insert_sorted grows a workspace with cudaMalloc and may free it again.
+ * A process that serves many streams cannot let a call do that (cudaMalloc
+ * and cudaFree can synchronize the whole device), a stream being captured into
+ * a CUDA graph may not allocate, and a host whose device memory is reserved by
+ * another allocator has none to give.  This entry point runs the same
+ * segment-staged insert on a fixed scratch area built into the library
+ * (cf_noalloc_scratch_bytes(), about 27 MiB), which every GPU that loads the
+ * library's device code holds until the process exits.  It calls no
+ * cudaMalloc, cudaFree or allocating routine.
+ *
+ * Limits: at most CF_NOALLOC_MAX_KEYS keys per call (larger n returns
+ * CF_ERR_INVALID; split the batch), tables of at most 2^18 segments of 64 KiB
+ * (16 GiB; else CF_ERR_UNSUPPORTED).  The first call on a device looks up the
+ * scratch address there; make that first call before any stream capture.
+ * All calls share the one scratch area: calls that overlap on the GPU (other
+ * streams, other threads, other filters) race and must be serialized by the
+ * caller.  Contract otherwise as cf_insert_sorted (synchronous; d_out and
+ * occupied_out optional).
+ */
+#define CF_NOALLOC_MAX_KEYS (1u << 20)
+int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,
+                             uint64_t* occupied_out);
+
+/* Bytes of the fixed scratch area used by cf_insert_sorted_noalloc. */
+uint64_t cf_noalloc_scratch_bytes(void);
+
 /* Lookups of this batch whose tag is in the primary bucket (one probe); the
  * rest take two probes.  Diagnostic for sector accounting. */
 int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* primary_hits, void* stream);
