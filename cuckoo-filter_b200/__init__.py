@@ -95,6 +95,7 @@ def library() -> C.CDLL:
     PF = C.POINTER(C.c_void_p)
     sig = {
         "cf_abi_version": ([], i32),
+        "cf_launch_count": ([], u64),
         "cf_last_error": ([], C.c_char_p),
         "cf_status_string": ([i32], C.c_char_p),
         "cf_config_supported": ([C.POINTER(_Config)], i32),
@@ -132,6 +133,11 @@ def library() -> C.CDLL:
         fn.restype = res
     _lib = L
     return L
+
+
+def launch_count() -> int:
+    """Kernels the library has launched since it was loaded."""
+    return int(library().cf_launch_count())
 
 
 def _check(status: int) -> None:

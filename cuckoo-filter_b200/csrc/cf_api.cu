@@ -392,6 +392,8 @@ extern "C" {
 
 int cf_abi_version(void) { return CF_ABI_VERSION; }
 
+uint64_t cf_launch_count(void) { return launch_counter().load(std::memory_order_relaxed); }
+
 const char* cf_last_error(void) { return g_err; }
 
 const char* cf_status_string(int status) {

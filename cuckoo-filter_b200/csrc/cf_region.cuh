@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_probe(DevTable t, const uint6
 // order), so the walk's only writes are sequential; k_rg_gather turns the
 // bits into per-key results.
 template <class C>
-__global__ void __launch_bounds__(kRgThreads, 3) k_rg_lookup(DevTable t, const uint64_t* __restrict__ ent, uint64_t m,
+__global__ void __launch_bounds__(kRgThreads) k_rg_lookup(DevTable t, const uint64_t* __restrict__ ent, uint64_t m,
                                                             uint32_t* __restrict__ hits) {
     constexpr int U = C::bucket_bytes > 32 ? 3 : C::bucket_bytes > 16 ? 6 : 8;  // bucket loads in flight per thread
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

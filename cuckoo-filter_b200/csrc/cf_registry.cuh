@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <vector>
 
@@ -16,6 +17,14 @@
 #include "cf_segmented.cuh"
 
 namespace cfb {
+
+// Kernels launched by this library since load (all filters, all devices);
+// read through cf_launch_count().
+inline std::atomic<unsigned long long>& launch_counter() {
+    static std::atomic<unsigned long long> c{0};
+    return c;
+}
+#define CF_COUNT_LAUNCH() (::cfb::launch_counter().fetch_add(1, std::memory_order_relaxed))
 
 // Geometry of the segment-staged path for one filter.
 struct SegGeom {
@@ -138,16 +147,16 @@ struct Launchers {
         if (n == 0) return cudaSuccess;
         constexpr int K = kContainsKPT;
         const int grid = grid_for(n, L.block, K, L.max_grid);
-        k_contains<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
-                                                         aligned(keys, key_vec_align<C, K>()), aligned(out, K));
+        { k_contains<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
+                                                         aligned(keys, key_vec_align<C, K>()), aligned(out, K)); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
     static cudaError_t remove(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
         if (n == 0) return cudaSuccess;
         constexpr int K = kDeleteKPT;
         const int grid = grid_for(n, L.block, K, L.max_grid);
-        k_delete<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
-                                                       aligned(keys, key_vec_align<C, K>()), aligned(out, K));
+        { k_delete<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
+                                                       aligned(keys, key_vec_align<C, K>()), aligned(out, K)); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
     static cudaError_t insert(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L,
@@ -155,21 +164,21 @@ struct Launchers {
         if (n == 0) return cudaSuccess;
         constexpr int K = kInsertKPT;
         const int grid = grid_for(n, L.block, K, L.max_grid);
-        k_insert<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
+        { k_insert<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
                                                        aligned(keys, key_vec_align<C, K>()), aligned(out, K),
-                                                       policy_bfs, max_ev);
+                                                       policy_bfs, max_ev); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
     static cudaError_t count(const DevTable& t, uint64_t nb, unsigned long long* result, const LaunchCfg& L) {
         const int grid = grid_for(nb, L.block, 1, L.max_grid);
-        k_count_occupied<C><<<grid, L.block, 0, L.stream>>>(t, nb, result);
+        { k_count_occupied<C><<<grid, L.block, 0, L.stream>>>(t, nb, result); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
     static cudaError_t probe(const DevTable& t, const void* keys, uint64_t n, unsigned long long* result,
                              const LaunchCfg& L) {
         if (n == 0) return cudaSuccess;
         const int grid = grid_for(n, L.block, 1, L.max_grid);
-        k_probe_count<C><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, result);
+        { k_probe_count<C><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, result); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
     static cudaError_t occupancy(int kid, int block, int* bps) {
@@ -200,28 +209,28 @@ struct Launchers {
         const void* hsrc = keys_mode ? src : static_cast<const void*>(ent_src);
         uint64_t* hout = keys_mode ? w.ent[1] : nullptr;
         if (keys_mode && lo_bits >= 0)
-            k_rs_hist<C, true, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
-                                                                     lo_bits, w.start);
+            { k_rs_hist<C, true, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
+                                                                     lo_bits, w.start); CF_COUNT_LAUNCH(); }
         else if (keys_mode)
-            k_rs_hist<C, true, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
-                                                                      0, nullptr);
+            { k_rs_hist<C, true, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
+                                                                      0, nullptr); CF_COUNT_LAUNCH(); }
         else if (lo_bits >= 0)
-            k_rs_hist<C, false, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
-                                                                      nullptr, lo_bits, w.start);
+            { k_rs_hist<C, false, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
+                                                                      nullptr, lo_bits, w.start); CF_COUNT_LAUNCH(); }
         else
-            k_rs_hist<C, false, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
-                                                                       nullptr, 0, nullptr);
-        k_scan_u32<<<1, 1024, 0, s>>>(w.hist, hist_n);
+            { k_rs_hist<C, false, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
+                                                                       nullptr, 0, nullptr); CF_COUNT_LAUNCH(); }
+        { k_scan_u32<<<1, 1024, 0, s>>>(w.hist, hist_n); CF_COUNT_LAUNCH(); }
         unsigned long long* err = t.ctr + CTR_ERROR;
         if (pay == 0)
-            k_rs_scatter<0><<<grid, kRsThreads, rs_scatter_smem<0>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
-                                                                          w.ent[dst], nullptr, err);
+            { k_rs_scatter<0><<<grid, kRsThreads, rs_scatter_smem<0>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
+                                                                          w.ent[dst], nullptr, err); CF_COUNT_LAUNCH(); }
         else if (pay == 1)
-            k_rs_scatter<1><<<grid, kRsThreads, rs_scatter_smem<1>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
-                                                                          w.ent[dst], w.pay[dst], err);
+            { k_rs_scatter<1><<<grid, kRsThreads, rs_scatter_smem<1>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
+                                                                          w.ent[dst], w.pay[dst], err); CF_COUNT_LAUNCH(); }
         else
-            k_rs_scatter<2><<<grid, kRsThreads, rs_scatter_smem<2>(), s>>>(ent_src, w.pay[from], n, nullptr, shift,
-                                                                          order_bits, w.hist, w.ent[dst], w.pay[dst], err);
+            { k_rs_scatter<2><<<grid, kRsThreads, rs_scatter_smem<2>(), s>>>(ent_src, w.pay[from], n, nullptr, shift,
+                                                                          order_bits, w.hist, w.ent[dst], w.pay[dst], err); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
 
@@ -247,7 +256,7 @@ struct Launchers {
             if (e != cudaSuccess) return e;
             cur = dst;
         }
-        if (count_segs) k_scan_u32<<<1, 1024, 0, s>>>(w.start, static_cast<uint32_t>(g.nseg + 1));
+        if (count_segs) { k_scan_u32<<<1, 1024, 0, s>>>(w.start, static_cast<uint32_t>(g.nseg + 1)); CF_COUNT_LAUNCH(); }
         *result = cur;
         *have_start = count_segs;
         return cudaGetLastError();
@@ -267,14 +276,14 @@ struct Launchers {
         if (!have_start) {
             const uint64_t bthreads = n / 8 + 1;  // 8 positions per thread
             const int bgrid = static_cast<int>((bthreads + 255) / 256 < 4096 ? (bthreads + 255) / 256 : 4096);
-            k_seg_bounds<<<bgrid, 256, 0, s>>>(w.ent[buf], n, nullptr, g.seg_shift, g.nseg, w.start);
+            { k_seg_bounds<<<bgrid, 256, 0, s>>>(w.ent[buf], n, nullptr, g.seg_shift, g.nseg, w.start); CF_COUNT_LAUNCH(); }
         }
         const int other = 1 - buf;
         // one wave: every resident CTA gets an equal share of the segments
         static const int bps = blocks_per_sm(kern, kSegThreads, kMaxSmem);
-        kern<<<w.sms * bps, kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start, g.nseg,
+        { kern<<<w.sms * bps, kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start, g.nseg,
                                                     g.sb_log2, round, w.ent[other], payload ? w.pay[other] : nullptr,
-                                                    &w.cnt[round - 1], payload ? w.bitmap : nullptr);
+                                                    &w.cnt[round - 1], payload ? w.bitmap : nullptr); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
 
@@ -305,28 +314,28 @@ struct Launchers {
                     static const int bfs_bps = blocks_per_sm(k_evict_bfs_steps<C>, 256, 0);
                     static const int list_bps = blocks_per_sm(k_evict_list<C>, 256, 0);
                     if (policy_bfs) {
-                        k_evict_bfs_steps<C><<<w.sms * bfs_bps, 256, 0, s>>>(t, w.ent[1 - c],
+                        { k_evict_bfs_steps<C><<<w.sms * bfs_bps, 256, 0, s>>>(t, w.ent[1 - c],
                                                                            payload ? w.pay[1 - c] : nullptr,
                                                                            &w.cnt[1], bm, w.ent[c],
-                                                                           payload ? w.pay[c] : nullptr, &w.cnt[2]);
-                        k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[c], payload ? w.pay[c] : nullptr,
-                                                                        &w.cnt[2], 0u, max_ev, bm, 1u);
+                                                                           payload ? w.pay[c] : nullptr, &w.cnt[2]); CF_COUNT_LAUNCH(); }
+                        { k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[c], payload ? w.pay[c] : nullptr,
+                                                                        &w.cnt[2], 0u, max_ev, bm, 1u); CF_COUNT_LAUNCH(); }
                     } else {
-                        k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[1 - c],
+                        { k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[1 - c],
                                                                         payload ? w.pay[1 - c] : nullptr, &w.cnt[1],
-                                                                        0u, max_ev, bm, 0u);
+                                                                        0u, max_ev, bm, 0u); CF_COUNT_LAUNCH(); }
                     }
                 }
             } else {
                 const int lgrid = static_cast<int>((m2 + 255) / 256 < 8192 ? (m2 + 255) / 256 : 8192);
-                k_list_random<C, OP><<<lgrid, 256, 0, s>>>(t, w.ent[b], payload ? w.pay[b] : nullptr, &w.cnt[0],
-                                                          policy_bfs, max_ev, payload ? w.bitmap : nullptr);
+                { k_list_random<C, OP><<<lgrid, 256, 0, s>>>(t, w.ent[b], payload ? w.pay[b] : nullptr, &w.cnt[0],
+                                                          policy_bfs, max_ev, payload ? w.bitmap : nullptr); CF_COUNT_LAUNCH(); }
             }
             if (e == cudaSuccess) e = cudaGetLastError();
         }
         if (e == cudaSuccess && payload) {
             const int xgrid = static_cast<int>(((m + 31) / 32 + 255) / 256 < 8192 ? ((m + 31) / 32 + 255) / 256 : 8192);
-            k_bitmap_expand<<<xgrid, 256, 0, s>>>(w.bitmap, m, out);
+            { k_bitmap_expand<<<xgrid, 256, 0, s>>>(w.bitmap, m, out); CF_COUNT_LAUNCH(); }
             e = cudaGetLastError();
         }
         return e;
@@ -348,14 +357,14 @@ struct Launchers {
                          const uint32_t* src_pay, uint64_t m, const unsigned long long* m_dev, bool payload,
                          uint64_t* dst, uint32_t* dst_pay, cudaStream_t s) {
         const int grid = w.rg_grid;
-        k_rg_hist<C, MODE><<<grid, kRgThreads, 0, s>>>(src, t.nb_mask, m, m_dev, g.rl, g.nreg, w.hist);
-        k_scan_u32<<<1, 1024, 0, s>>>(w.hist, g.nreg * static_cast<uint32_t>(grid));
+        { k_rg_hist<C, MODE><<<grid, kRgThreads, 0, s>>>(src, t.nb_mask, m, m_dev, g.rl, g.nreg, w.hist); CF_COUNT_LAUNCH(); }
+        { k_scan_u32<<<1, 1024, 0, s>>>(w.hist, g.nreg * static_cast<uint32_t>(grid)); CF_COUNT_LAUNCH(); }
         if (payload)
-            k_rg_scatter<C, MODE, true><<<grid, kRgThreads, 0, s>>>(src, src_pay, t.nb_mask, m, m_dev, g.rl, g.nreg,
-                                                                    w.hist, dst, dst_pay);
+            { k_rg_scatter<C, MODE, true><<<grid, kRgThreads, 0, s>>>(src, src_pay, t.nb_mask, m, m_dev, g.rl, g.nreg,
+                                                                    w.hist, dst, dst_pay); CF_COUNT_LAUNCH(); }
         else
-            k_rg_scatter<C, MODE, false><<<grid, kRgThreads, 0, s>>>(src, nullptr, t.nb_mask, m, m_dev, g.rl, g.nreg,
-                                                                     w.hist, dst, nullptr);
+            { k_rg_scatter<C, MODE, false><<<grid, kRgThreads, 0, s>>>(src, nullptr, t.nb_mask, m, m_dev, g.rl, g.nreg,
+                                                                     w.hist, dst, nullptr); CF_COUNT_LAUNCH(); }
     }
 
     template <int OP>
@@ -363,8 +372,8 @@ struct Launchers {
                          const unsigned long long* m_dev, int round, uint64_t* next, uint32_t* next_pay,
                          unsigned long long* next_count, uint32_t* bitmap, cudaStream_t s) {
         static const int bps = blocks_per_sm(k_rg_probe<C, OP>, kRgThreads, 0);
-        k_rg_probe<C, OP><<<w.sms * bps, kRgThreads, 0, s>>>(t, ent, pay, m, m_dev, round, next, next_pay, next_count,
-                                                            bitmap);
+        { k_rg_probe<C, OP><<<w.sms * bps, kRgThreads, 0, s>>>(t, ent, pay, m, m_dev, round, next, next_pay, next_count,
+                                                            bitmap); CF_COUNT_LAUNCH(); }
     }
 
     // A chunk of m keys through the region-staged path.  Lookups: one pass
@@ -385,14 +394,14 @@ struct Launchers {
             // order (w.bitmap, 2m bits); per-chunk gather writes `out`
             rg_split<RG_KEYS_DUAL>(t, g, w, keys, nullptr, m, nullptr, true, w.ent[0], w.pay[0], s);
             static const int lk_bps = blocks_per_sm(k_rg_lookup<C>, kRgThreads, 0);
-            k_rg_lookup<C><<<w.sms * lk_bps, kRgThreads, 0, s>>>(t, w.ent[0], 2 * m, w.bitmap);
+            { k_rg_lookup<C><<<w.sms * lk_bps, kRgThreads, 0, s>>>(t, w.ent[0], 2 * m, w.bitmap); CF_COUNT_LAUNCH(); }
             e = ensure_smem_attr<k_rg_gather>(kRgGatherMaxSmem);
             if (e != cudaSuccess) return e;
             const uint64_t per = (m + w.rg_grid - 1) / w.rg_grid;
             const uint64_t chunk = (per + kRgTile / 2 - 1) / (kRgTile / 2) * (kRgTile / 2);
             const int smem = static_cast<int>((chunk + 31) / 32 * 4);
             if (smem > kRgGatherMaxSmem) return cudaErrorInvalidValue;
-            k_rg_gather<<<w.rg_grid, kRgThreads, smem, s>>>(w.pay[0], w.bitmap, w.hist, g.nreg, m, 2 * m, out);
+            { k_rg_gather<<<w.rg_grid, kRgThreads, smem, s>>>(w.pay[0], w.bitmap, w.hist, g.nreg, m, 2 * m, out); CF_COUNT_LAUNCH(); }
             return cudaGetLastError();
         } else {
             uint32_t* p0 = payload ? w.pay[0] : nullptr;
@@ -407,18 +416,18 @@ struct Launchers {
                 static const int bfs_bps = blocks_per_sm(k_evict_bfs_steps<C>, 256, 0);
                 static const int list_bps = blocks_per_sm(k_evict_list<C>, 256, 0);
                 if (policy_bfs) {
-                    k_evict_bfs_steps<C><<<w.sms * bfs_bps, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], bm, w.ent[0], p0,
-                                                                       &w.cnt[2]);
-                    k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[0], p0, &w.cnt[2], 0u, max_ev, bm, 1u);
+                    { k_evict_bfs_steps<C><<<w.sms * bfs_bps, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], bm, w.ent[0], p0,
+                                                                       &w.cnt[2]); CF_COUNT_LAUNCH(); }
+                    { k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[0], p0, &w.cnt[2], 0u, max_ev, bm, 1u); CF_COUNT_LAUNCH(); }
                 } else {
-                    k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], 0u, max_ev, bm, 0u);
+                    { k_evict_list<C><<<w.sms * list_bps, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], 0u, max_ev, bm, 0u); CF_COUNT_LAUNCH(); }
                 }
             }
         }
         e = cudaGetLastError();
         if (e == cudaSuccess && payload) {
             const int xgrid = static_cast<int>(((m + 31) / 32 + 255) / 256 < 8192 ? ((m + 31) / 32 + 255) / 256 : 8192);
-            k_bitmap_expand<<<xgrid, 256, 0, s>>>(w.bitmap, m, out);
+            { k_bitmap_expand<<<xgrid, 256, 0, s>>>(w.bitmap, m, out); CF_COUNT_LAUNCH(); }
             e = cudaGetLastError();
         }
         return e;

@@ -88,6 +88,10 @@ typedef struct cf_stats {
 /* Library ABI version (CF_ABI_VERSION). */
 int cf_abi_version(void);
 
+/* Kernels this library has launched since it was loaded (all filters, all
+ * devices; a diagnostic counter). */
+uint64_t cf_launch_count(void);
+
 /* Message for the last failed call on this thread ("" if none). */
 const char* cf_last_error(void);
 
