@@ -270,26 +270,33 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(world, x: float) -> float:
+def _reduce(world, x: float, op: str) -> float:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(world, x: float) -> float:
+    return _reduce(world, x, "max")
 
 
 def sum_over_ranks(world, x: float) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    return _reduce(world, x, "sum")
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+
+def aggregate(world, keys_per_step: int, steps: int, total_ms: float) -> tuple[float, float]:
+    """Whole-job throughput: keys processed by all ranks (each rank owns an
+    independent filter shard) over the slowest rank's device time.  Returns
+    (Gkeys/s, max total ms)."""
+    total_ms_max = max_over_ranks(world, total_ms)
+    all_keys = sum_over_ranks(world, keys_per_step * steps)
+    return all_keys / (total_ms_max / 1e3) / 1e9, total_ms_max
 
 
 # ------------------------------------------------------------ CPU baselines
@@ -424,10 +431,9 @@ def run_b200(args, w: dict) -> dict | None:
     con_ms = [evs[k][2].elapsed_time(evs[k][3]) for k in range(args.steps)]
     del_ms = [evs[k][3].elapsed_time(evs[k][4]) for k in range(args.steps)]
     total_ms = sum(step_ms)
-    total_ms_max = max_over_ranks(world, total_ms)
     keys_per_step = n_fill + n_q + n_d
-    all_keys = sum_over_ranks(world, keys_per_step * args.steps)
-    value = all_keys / (total_ms_max / 1e3) / 1e9
+    value, total_ms_max = aggregate(world, keys_per_step, args.steps, total_ms)
+    all_keys = value * 1e9 * total_ms_max / 1e3
 
     peak, peak_src = measured_peak()
     ins_bytes = n_fill * (8 + 32 + 32) + 32 * acct["i1_full"]
