@@ -121,6 +121,21 @@ def library() -> C.CDLL:
         "cf_probe_count": ([vp, vp, u64, P64, vp], i32),
         "cf_hash_candidates": ([C.POINTER(_Config), u64, vp, u64, vp, vp, vp], i32),
         "cf_hash64": ([u32, vp, u64, vp], i32),
+        "cf_set_create": ([C.POINTER(_Config), u32, vp, PF], i32),
+        "cf_set_destroy": ([vp], i32),
+        "cf_set_size": ([vp, C.POINTER(C.c_uint32), P64], i32),
+        "cf_set_get_info": ([vp, u32, C.POINTER(_Info)], i32),
+        "cf_set_table": ([vp, u32, PF, P64], i32),
+        "cf_set_insert_async": ([vp, vp, u64, vp, vp, u32, vp, vp], i32),
+        "cf_set_contains_async": ([vp, vp, u64, vp, vp, u32, vp, vp], i32),
+        "cf_set_delete_async": ([vp, vp, u64, vp, vp, u32, vp, vp], i32),
+        "cf_set_sync": ([vp, vp], i32),
+        "cf_set_clear": ([vp, vp], i32),
+        "cf_set_occupied": ([vp, vp], i32),
+        "cf_set_get_stats": ([vp, u32, C.POINTER(_Stats)], i32),
+        "cf_set_set_launch": ([vp, i32, u32, u32, u32], i32),
+        "cf_set_get_launch": ([vp, i32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)], i32),
+        "cf_set_autotune": ([vp, i32, vp, u64, vp, vp, u32, vp, vp, C.POINTER(C.c_float)], i32),
         "cf_insert_sorted_noalloc": ([vp, vp, u64, vp, vp, P64], i32),
         "cf_noalloc_scratch_bytes": ([], u64),
         "cf_alt_buckets": ([C.POINTER(_Config), u64, vp, vp, u64, vp], i32),
@@ -407,4 +422,144 @@ class CuckooFilter:
         return i1, i2, fp
 
 
-__all__ = ["CuckooConfig", "CuckooFilter", "EvictionPolicy", "CuckooError", "library", "LIB_PATH"]
+SET_INSERT, SET_CONTAINS, SET_DELETE = 0, 1, 2
+
+
+class CuckooFilterSet:
+    """Many independent filters of one configuration, batched (cf_set_* ABI).
+
+    A batched call takes the concatenated keys of all items plus a device work
+    list: ``offsets`` (int64, n_items + 1 entries, offsets[-1] == len(keys))
+    and ``filters`` (int32, n_items): item j is keys[offsets[j]:offsets[j+1]]
+    for filter filters[j].  Every item runs in one kernel launch.  The
+    ``*_async`` methods only enqueue (capturable in a CUDA graph); ``sync()``
+    waits and raises on device-side errors.
+    """
+
+    def __init__(self, config: CuckooConfig, capacities):
+        import numpy as np
+
+        self.config = config
+        caps = np.ascontiguousarray(np.asarray(capacities, dtype=np.uint64))
+        h = C.c_void_p()
+        c = config.to_c()
+        _check(library().cf_set_create(C.byref(c), len(caps), caps.ctypes.data, C.byref(h)))
+        self._h = h
+        self.n = len(caps)
+        info = _Info()
+        self.num_buckets = []
+        self.capacities = []
+        for i in range(self.n):
+            _check(library().cf_set_get_info(self._h, i, C.byref(info)))
+            self.num_buckets.append(int(info.num_buckets))
+            self.capacities.append(int(info.capacity))
+        self.device = int(info.device)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            library().cf_set_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return int(self._h.value or 0)
+
+    def _args(self, keys, offsets, filters, out):
+        kp, n = _dev_ptr(keys, None, 8, "keys")
+        op, no = _dev_ptr(offsets, None, 8, "offsets")
+        fp, nf = _dev_ptr(filters, None, 4, "filters")
+        if no != nf + 1:
+            raise ValueError("offsets must have len(filters) + 1 entries")
+        optr = 0 if out is None else _dev_ptr(out, n, 1, "out")[0]
+        return kp, n, op, fp, nf, optr or None
+
+    def insert_async(self, keys, offsets, filters, out=None, stream=None) -> None:
+        kp, n, op, fp, nf, optr = self._args(keys, offsets, filters, out)
+        _check(library().cf_set_insert_async(self._h, kp, n, op, fp, nf, optr, _stream_handle(stream)))
+
+    def contains_async(self, keys, offsets, filters, out, stream=None) -> None:
+        kp, n, op, fp, nf, optr = self._args(keys, offsets, filters, out)
+        _check(library().cf_set_contains_async(self._h, kp, n, op, fp, nf, optr, _stream_handle(stream)))
+
+    def delete_async(self, keys, offsets, filters, out=None, stream=None) -> None:
+        kp, n, op, fp, nf, optr = self._args(keys, offsets, filters, out)
+        _check(library().cf_set_delete_async(self._h, kp, n, op, fp, nf, optr, _stream_handle(stream)))
+
+    def sync(self, stream=None) -> None:
+        _check(library().cf_set_sync(self._h, _stream_handle(stream)))
+
+    def clear(self, stream=None) -> None:
+        _check(library().cf_set_clear(self._h, _stream_handle(stream)))
+
+    def occupied(self):
+        import numpy as np
+
+        out = np.zeros(self.n, np.uint64)
+        _check(library().cf_set_occupied(self._h, out.ctypes.data))
+        return out
+
+    def stats(self, i: int) -> dict:
+        st = _Stats()
+        _check(library().cf_set_get_stats(self._h, i, C.byref(st)))
+        return {name: int(getattr(st, name)) for name, _ in _Stats._fields_}
+
+    def table(self, i: int):
+        p = C.c_void_p()
+        b = C.c_uint64()
+        _check(library().cf_set_table(self._h, i, C.byref(p), C.byref(b)))
+        return int(p.value or 0), int(b.value)
+
+    def table_view(self, i: int):
+        """Filter i's table image as a uint8 CUDA tensor viewing the set's pool
+        (no copy; valid while the set lives)."""
+        ptr, nbytes = self.table(i)
+        return _device_view(ptr, nbytes, self.device)
+
+    def table_image(self, i: int):
+        """Copy of filter i's table image as a uint8 CPU tensor."""
+        return self.table_view(i).cpu()
+
+    def load_table(self, i: int, image) -> None:
+        """Replace filter i's table with an image (CPU or CUDA uint8 tensor).
+        Counters are not recomputed."""
+        view = self.table_view(i)
+        if image.numel() != view.numel():
+            raise ValueError(f"image is {image.numel()} bytes, table is {view.numel()}")
+        view.copy_(image)
+        _torch().cuda.synchronize(self.device)
+
+    def set_launch(self, op: int, block: int, kpt: int, width: int = 1) -> None:
+        _check(library().cf_set_set_launch(self._h, op, block, kpt, width))
+
+    def get_launch(self, op: int):
+        b, k, w = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(library().cf_set_get_launch(self._h, op, C.byref(b), C.byref(k), C.byref(w)))
+        return int(b.value), int(k.value), int(w.value)
+
+    def autotune(self, op: int, keys, offsets, filters, out=None, stream=None) -> float:
+        kp, n, opp, fp, nf, optr = self._args(keys, offsets, filters, out)
+        best = C.c_float()
+        _check(library().cf_set_autotune(self._h, op, kp, n, opp, fp, nf, optr, _stream_handle(stream),
+                                         C.byref(best)))
+        return float(best.value)
+
+
+class _DeviceBuffer:
+    """Raw device memory exposed through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 2}
+
+
+def _device_view(ptr: int, nbytes: int, device: int):
+    torch = _torch()
+    return torch.as_tensor(_DeviceBuffer(ptr, nbytes), device=f"cuda:{device}")
+
+
+__all__ = ["CuckooConfig", "CuckooFilter", "CuckooFilterSet", "EvictionPolicy", "CuckooError", "library", "LIB_PATH"]

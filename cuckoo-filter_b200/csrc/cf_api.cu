@@ -388,6 +388,14 @@ void host_candidates(uint32_t kb, uint32_t bits, uint64_t mask, const void* keys
 
 }  // namespace
 
+namespace cfb {
+// Error reporting for the other translation units of the C ABI (filter sets).
+int api_fail(int status, const char* msg) { return fail(status, "%s", msg); }
+int api_cuda_fail(cudaError_t e, const char* what) { return cuda_fail(e, what); }
+int api_validate(const cf_config* cfg) { return validate(cfg); }
+uint64_t api_num_buckets(uint64_t capacity, uint32_t bucket_size) { return num_buckets_for(capacity, bucket_size); }
+}  // namespace cfb
+
 extern "C" {
 
 int cf_abi_version(void) { return CF_ABI_VERSION; }

@@ -272,6 +272,65 @@ uint64_t cf_noalloc_scratch_bytes(void);
  * rest take two probes.  Diagnostic for sector accounting. */
 int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* primary_hits, void* stream);
 
+/*
+ * ------------------------------------------------------------- filter sets
+ *
+ * Batched form over many filters (an extension; the reference runs one filter
+ * per object and one launch per batch, CuckooFilter.cuh:457-548).  A set holds
+ * n_filters independent filters of one configuration (64-bit keys; 8/16, 16/16
+ * or 32/8 bits per tag / bucket size), each with its own capacity and its own
+ * counters, tables in one device pool.  A batched call takes a device work
+ * list: item j covers keys [d_offsets[j], d_offsets[j+1]) of the concatenated
+ * key buffer and targets filter d_filters[j]; d_offsets has n_items + 1
+ * monotonic entries with d_offsets[n_items] = n, and d_out (when given) is
+ * aligned with the keys.  All items run in ONE persistent kernel.  The
+ * *_async calls only launch (no allocation, no synchronization), so they can
+ * be captured into a CUDA graph and replayed; cf_set_sync synchronizes and
+ * reports device-side errors (an item naming a filter outside the set: its
+ * keys are skipped, CF_ERR_INVALID).
+ */
+typedef struct cf_set cf_set;
+
+typedef enum cf_set_op { CF_SET_OP_INSERT = 0, CF_SET_OP_CONTAINS = 1, CF_SET_OP_DELETE = 2 } cf_set_op;
+
+int cf_set_create(const cf_config* cfg, uint32_t n_filters, const uint64_t* capacities, cf_set** out);
+int cf_set_destroy(cf_set* s);
+/* Number of filters and bytes of the table pool. */
+int cf_set_size(const cf_set* s, uint32_t* n_filters, uint64_t* pool_bytes);
+int cf_set_get_info(const cf_set* s, uint32_t i, cf_info* out);
+/* Device pointer and size of filter i's table image (layout as cf_table). */
+int cf_set_table(cf_set* s, uint32_t i, void** d_table, uint64_t* bytes);
+
+/* insertMany / containsMany / deleteMany of every item, one launch each. */
+int cf_set_insert_async(cf_set* s, const void* d_keys, uint64_t n, const uint64_t* d_offsets,
+                        const uint32_t* d_filters, uint32_t n_items, uint8_t* d_out, void* stream);
+int cf_set_contains_async(cf_set* s, const void* d_keys, uint64_t n, const uint64_t* d_offsets,
+                          const uint32_t* d_filters, uint32_t n_items, uint8_t* d_out, void* stream);
+int cf_set_delete_async(cf_set* s, const void* d_keys, uint64_t n, const uint64_t* d_offsets,
+                        const uint32_t* d_filters, uint32_t n_items, uint8_t* d_out, void* stream);
+int cf_set_sync(cf_set* s, void* stream);
+
+/* Zero every table and counter (synchronous). */
+int cf_set_clear(cf_set* s, void* stream);
+/* occupiedSlots() of every filter into out[n_filters]. */
+int cf_set_occupied(cf_set* s, uint64_t* out);
+int cf_set_get_stats(cf_set* s, uint32_t i, cf_stats* out);
+
+/* Launch shape of an operation: threads per block (multiple of 32, <= 512),
+ * keys per thread (1, 2, 4, 8) and, for lookups, the probe width (1 = one
+ * thread per key; 4 or 8 lanes per key, each loading a 4- or 8-byte piece of
+ * the bucket, where the bucket splits that way). */
+int cf_set_set_launch(cf_set* s, int op, uint32_t block, uint32_t kpt, uint32_t width);
+int cf_set_get_launch(const cf_set* s, int op, uint32_t* block, uint32_t* kpt, uint32_t* width);
+
+/* Autotuner: times every launch shape (blocks {128, 256, 512} x keys per
+ * thread {1, 2, 4, 8} x probe widths {1, 4, 8} for lookups) on the given batch
+ * and keeps the fastest for `op`.  Lookups leave the set unchanged; tuning
+ * inserts or deletes clears the set (each trial starts from an empty set) and
+ * leaves it empty.  *best_ms (optional) receives the best trial's time. */
+int cf_set_autotune(cf_set* s, int op, const void* d_keys, uint64_t n, const uint64_t* d_offsets,
+                    const uint32_t* d_filters, uint32_t n_items, uint8_t* d_out, void* stream, float* best_ms);
+
 #ifdef __cplusplus
 }
 #endif
