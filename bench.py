@@ -614,6 +614,144 @@ def load_traffic(op: str, w: dict, path: str) -> dict | None:
     return {"bytes_per_launch": e["bytes_per_key"] * n, "source": e.get("source", p)}
 
 
+# ------------------------------------------------------------ batched form
+
+
+def splitmix64_segments(seeds, counts, first, device):
+    """Concatenation over i of splitmix64(seeds[i]) outputs first[i] ..
+    first[i] + counts[i] - 1, as one int64 tensor (one vectorised pass)."""
+    import torch
+
+    seeds_t = torch.as_tensor(seeds, dtype=torch.int64, device=device)
+    counts_t = torch.as_tensor(counts, dtype=torch.int64, device=device)
+    first_t = torch.as_tensor(first, dtype=torch.int64, device=device)
+    seg = torch.repeat_interleave(torch.arange(len(counts), device=device), counts_t)
+    starts = torch.cumsum(counts_t, 0) - counts_t
+    pos = torch.arange(int(counts_t.sum().item()), device=device, dtype=torch.int64) - starts[seg] + first_t[seg]
+
+    def lsr(z, sh):
+        return (z >> sh) & ((1 << (64 - sh)) - 1)
+
+    z = (pos + 1) * s64(G) + seeds_t[seg]
+    z = (z ^ lsr(z, 30)) * s64(M1)
+    z = (z ^ lsr(z, 27)) * s64(M2)
+    return z ^ lsr(z, 31)
+
+
+def run_batched(args) -> dict:
+    """Batched form: 4096 filters with capacities log-uniform in 2^10..2^22
+    slots (16-bit tags, 16-slot buckets), key batches lognormal(ln 20000, 1.5)
+    clipped to 0.9 of capacity, keys splitmix64(seed = filter id).  All inserts
+    in one launch, then all lookups (50 % positive) replayed from a captured
+    CUDA graph; against a loop of per-filter insertMany / containsMany calls."""
+    import numpy as np
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(args.batched_seed)
+    nf = args.filters
+    caps = np.exp2(rng.uniform(10, 22, nf)).astype(np.uint64)
+    sizes = np.minimum(rng.lognormal(np.log(20000), 1.5, nf), 0.9 * caps).astype(np.int64)
+    ids = np.arange(nf, dtype=np.int64)
+    keys = splitmix64_segments(ids, sizes, np.zeros(nf, np.int64), dev)
+    offs = torch.zeros(nf + 1, dtype=torch.int64, device=dev)
+    offs[1:] = torch.cumsum(torch.as_tensor(sizes, device=dev), 0)
+    filt = torch.arange(nf, dtype=torch.int32, device=dev)
+    # lookups: per filter, the first half of its batch (positives) + as many keys of another stream
+    npos = sizes // 2
+    nneg = sizes - npos
+    pos = splitmix64_segments(ids, npos, np.zeros(nf, np.int64), dev)
+    neg = splitmix64_segments(ids + (1 << 40), nneg, np.zeros(nf, np.int64), dev)
+    qs = torch.cat([torch.cat([p, q]) for p, q in zip(pos.split(npos.tolist()), neg.split(nneg.tolist()))])
+    qoffs = offs  # same sizes per filter
+    n_keys, n_q = int(sizes.sum()), int(sizes.sum())
+    q_out = torch.empty(n_q, dtype=torch.uint8, device=dev)
+    cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16, bucketSize=16, maxEvictions=500,
+                           evictionPolicy=cfb.EvictionPolicy.BFS)
+    stream = torch.cuda.Stream(device=dev)
+    s = cfb.CuckooFilterSet(cfg, caps)
+    # autotune inserts (clears the set), then fill and autotune lookups on the filled set
+    t_ins_tune = s.autotune(cfb.SET_INSERT, keys, offs, filt, stream=stream)
+    s.insert_async(keys, offs, filt, stream=stream)
+    s.sync(stream=stream)
+    t_con_tune = s.autotune(cfb.SET_CONTAINS, qs, qoffs, filt, q_out, stream=stream)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        s.contains_async(qs, qoffs, filt, q_out, stream=stream)
+    torch.cuda.synchronize()
+    ins_ms, con_ms = [], []
+    for k in range(args.warmup + args.steps):
+        s.clear(stream=stream)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        s.insert_async(keys, offs, filt, stream=stream)
+        e[1].record(stream)
+        with torch.cuda.stream(stream):  # replay on the stream the events are recorded on
+            g.replay()
+        e[2].record(stream)
+        s.sync(stream=stream)
+        if k >= args.warmup:
+            ins_ms.append(e[0].elapsed_time(e[1]))
+            con_ms.append(e[1].elapsed_time(e[2]))
+    occ = s.occupied()
+    set_hits = int(q_out.sum().item())
+    pos_found = all(bool(q_out[int(o):int(o) + int(p)].all().item()) for o, p in
+                    zip(offs[:-1].tolist()[:64], npos[:64]))  # spot check of the first 64 filters
+    # baseline: a loop of per-filter calls of the plain API (synchronous, as the reference's API is)
+    filters = [cfb.CuckooFilter(cfg, int(c)) for c in caps]
+    kh = keys.split(sizes.tolist())
+    qh = qs.split(sizes.tolist())
+    outs = q_out.split(sizes.tolist())
+    loop_ins, loop_con = [], []
+    for k in range(max(1, min(args.steps, 2)) + 1):
+        for f in filters:
+            f.clear(stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for f, kk in zip(filters, kh):
+            f.insertMany(kk, stream=stream)
+        t1 = time.perf_counter()
+        for f, qq, oo in zip(filters, qh, outs):
+            f.containsMany(qq, oo, stream=stream)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if k:
+            loop_ins.append(t1 - t0)
+            loop_con.append(t2 - t1)
+    loop_hits = int(q_out.sum().item())
+    ti, tc = statistics.mean(ins_ms) / 1e3, statistics.mean(con_ms) / 1e3
+    li, lc = statistics.mean(loop_ins), statistics.mean(loop_con)
+    res = {
+        "form": "batched", "metric": "Gkeys/s aggregate insert + lookup over 4096 uneven filters",
+        "value": (n_keys + n_q) / (ti + tc) / 1e9, "unit": "Gkeys/s", "higher_is_better": True, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "u64", "data": "synthetic: splitmix64(seed = filter id)",
+        "config": {"workload": "batched: 4096 filters, capacities log-uniform 2^10..2^22 slots, 16/16, BFS; batches "
+                               "lognormal(ln 20000, 1.5) clipped to 0.9 capacity; lookups 50% positive",
+                   "filters": nf, "insert_keys": n_keys, "lookup_keys": n_q,
+                   "table_bytes": int(sum(n * 32 for n in s.num_buckets))},
+        "set": {"insert_gkeys_s": n_keys / ti / 1e9, "insert_ms": ti * 1e3, "lookup_gkeys_s": n_q / tc / 1e9,
+                "lookup_ms": tc * 1e3, "launches_per_step": 2, "insert_launch": s.get_launch(cfb.SET_INSERT),
+                "lookup_launch": s.get_launch(cfb.SET_CONTAINS), "tune_best_ms": {"insert": t_ins_tune,
+                                                                                 "lookup": t_con_tune},
+                "lookup_path": "one CUDA-graph replay", "hits": set_hits, "occupied": int(occ.sum()),
+                "positives_found_spot_check": pos_found},
+        "loop_baseline": {"insert_gkeys_s": n_keys / li / 1e9, "insert_ms": li * 1e3,
+                          "lookup_gkeys_s": n_q / lc / 1e9, "lookup_ms": lc * 1e3,
+                          "value": (n_keys + n_q) / (li + lc) / 1e9, "hits": loop_hits,
+                          "path": "4096 synchronous insertMany calls, then 4096 containsMany calls; wall clock"},
+        "speedup_vs_loop": (li + lc) / (ti + tc),
+    }
+    del g
+    for f in filters:
+        f.close()
+    s.close()
+    return res
+
+
 # ------------------------------------------------------------ reference arm
 
 
@@ -717,11 +855,18 @@ def main() -> None:
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--cpu-scale", type=int, default=27, help="log2 slots of the CPU-baseline sample")
     ap.add_argument("--ref-scale", type=int, default=25, help="log2 slots of each reference-arm CPU step")
+    ap.add_argument("--form", choices=("plain", "batched"), default="plain",
+                    help="batched: the filter-set form over 4096 uneven filters (its own JSON line)")
+    ap.add_argument("--filters", type=int, default=4096)
+    ap.add_argument("--batched-seed", type=int, default=1)
     args = ap.parse_args()
     if args.warmup < 1:
         ap.error("--warmup must be >= 1")
     w = WORKLOADS[args.workload]
-    res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
+    if args.form == "batched":
+        res = run_batched(args)
+    else:
+        res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
     if res is not None:
         print(json.dumps(res), flush=True)
 

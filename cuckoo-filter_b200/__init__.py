@@ -50,6 +50,8 @@ OPT_REGION_MIN_KEYS = 5
 OPT_STAGING = 6
 OPT_REGION_BYTES = 7
 OPT_REGION_COUNT = 8
+OPT_LOOKUP_KPT = 9
+OPT_PERSISTENT = 10
 NEVER = (1 << 64) - 1
 
 # cf_staging values (OPT_STAGING)

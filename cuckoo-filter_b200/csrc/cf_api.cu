@@ -47,6 +47,8 @@ struct cf_filter {
     uint64_t rg_min_keys;   // CF_OPT_REGION_MIN_KEYS (0 = automatic)
     uint32_t staging;       // CF_OPT_STAGING (cf_staging)
     uint64_t rg_bytes;      // CF_OPT_REGION_BYTES (0 = kRgRegionBytes)
+    uint32_t lookup_kpt;    // CF_OPT_LOOKUP_KPT (0 = default)
+    uint32_t persistent;    // CF_OPT_PERSISTENT (0 = one tile per CTA, 1 = persistent grid)
 };
 
 namespace {
@@ -130,7 +132,9 @@ uint64_t num_buckets_for(uint64_t capacity, uint32_t bucket_size) {
 DevTable dev(const cf_filter* f) { return DevTable{f->d_table, f->num_buckets - 1, f->d_ctr}; }
 
 LaunchCfg launch(const cf_filter* f, int kid, void* stream) {
-    return LaunchCfg{static_cast<cudaStream_t>(stream), f->block, f->max_grid[kid]};
+    LaunchCfg L{static_cast<cudaStream_t>(stream), f->block, f->max_grid[kid]};
+    L.full_grid = f->persistent == 0;
+    return L;
 }
 
 LaunchCfg launch_aux(const cf_filter* f, void* stream) {
@@ -530,7 +534,9 @@ int cf_contains_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_o
         case PATH_SEGMENT: return run_segmented(f, SEG_CONTAINS, d_keys, n, d_out, stream);
         default: break;
     }
-    CF_CUDA(f->ops->contains(dev(f), d_keys, n, d_out, launch(f, KID_CONTAINS, stream)), "contains launch");
+    LaunchCfg L = launch(f, KID_CONTAINS, stream);
+    L.kpt = static_cast<int>(f->lookup_kpt);
+    CF_CUDA(f->ops->contains(dev(f), d_keys, n, d_out, L), "contains launch");
     return CF_OK;
 }
 
@@ -662,6 +668,15 @@ int cf_set_option(cf_filter* f, int option, uint64_t value) {
                                                        static_cast<unsigned long long>(value));
             f->staging = static_cast<uint32_t>(value);
             return CF_OK;
+        case CF_OPT_LOOKUP_KPT:
+            if (value != 0 && value != 1 && value != 2 && value != 4)
+                return fail(CF_ERR_INVALID, "lookup keys per thread must be 0, 1, 2 or 4");
+            f->lookup_kpt = static_cast<uint32_t>(value);
+            return CF_OK;
+        case CF_OPT_PERSISTENT:
+            if (value > 1) return fail(CF_ERR_INVALID, "persistent must be 0 or 1");
+            f->persistent = static_cast<uint32_t>(value);
+            return CF_OK;
         case CF_OPT_REGION_BYTES:
             if (value & (value - 1)) return fail(CF_ERR_INVALID, "region bytes must be 0 or a power of two");
             f->rg_bytes = value;
@@ -684,6 +699,8 @@ int cf_get_option(cf_filter* f, int option, uint64_t* value) {
         case CF_OPT_STAGING: *value = f->staging; return CF_OK;
         case CF_OPT_REGION_BYTES: *value = f->rg_bytes ? f->rg_bytes : kRgRegionBytes; return CF_OK;
         case CF_OPT_REGION_COUNT: *value = f->rgeom.nreg; return CF_OK;
+        case CF_OPT_LOOKUP_KPT: *value = f->lookup_kpt; return CF_OK;
+        case CF_OPT_PERSISTENT: *value = f->persistent; return CF_OK;
         default: return fail(CF_ERR_INVALID, "unknown option %d", option);
     }
 }

@@ -69,7 +69,9 @@ enum KernelId : int { KID_CONTAINS = 0, KID_DELETE = 1, KID_INSERT = 2, KID_COUN
 struct LaunchCfg {
     cudaStream_t stream;
     int block;
-    int max_grid;  // persistent grid for this kernel and block size
+    int max_grid;        // persistent grid for this kernel and block size
+    int kpt = 0;         // keys per thread of the lookup kernel (1, 2, 4; 0 = kContainsKPT)
+    bool full_grid = true;   // one tile per CTA instead of a persistent grid
 };
 
 struct OpsTable {
@@ -128,6 +130,14 @@ cudaError_t rs_scatter_grid(int sms, int* grid) {
     return cudaSuccess;
 }
 
+// One tile of block * kpt keys per CTA (kernels still stride if the batch
+// needs more than 2^31 - 1 CTAs).
+inline int full_grid_for(uint64_t n, int block, int kpt) {
+    const uint64_t tile = static_cast<uint64_t>(block) * kpt;
+    const uint64_t tiles = (n + tile - 1) / tile;
+    return static_cast<int>(tiles < 0x7FFFFFFFull ? tiles : 0x7FFFFFFFull);
+}
+
 inline int grid_for(uint64_t n, int block, int kpt, int max_grid) {
     const uint64_t tile = static_cast<uint64_t>(block) * kpt;
     const uint64_t tiles = (n + tile - 1) / tile;
@@ -143,18 +153,25 @@ template <class C>
 struct Launchers {
     using Key = typename C::Key;
 
-    static cudaError_t contains(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
-        if (n == 0) return cudaSuccess;
-        constexpr int K = kContainsKPT;
-        const int grid = grid_for(n, L.block, K, L.max_grid);
+    template <int K>
+    static cudaError_t contains_k(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
+        const int grid = L.full_grid ? full_grid_for(n, L.block, K) : grid_for(n, L.block, K, L.max_grid);
         { k_contains<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
                                                          aligned(keys, key_vec_align<C, K>()), aligned(out, K)); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
+    static cudaError_t contains(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
+        if (n == 0) return cudaSuccess;
+        switch (L.kpt) {
+            case 1: return contains_k<1>(t, keys, n, out, L);
+            case 2: return contains_k<2>(t, keys, n, out, L);
+            default: return contains_k<kContainsKPT>(t, keys, n, out, L);
+        }
+    }
     static cudaError_t remove(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
         if (n == 0) return cudaSuccess;
         constexpr int K = kDeleteKPT;
-        const int grid = grid_for(n, L.block, K, L.max_grid);
+        const int grid = L.full_grid ? full_grid_for(n, L.block, K) : grid_for(n, L.block, K, L.max_grid);
         { k_delete<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
                                                        aligned(keys, key_vec_align<C, K>()), aligned(out, K)); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
@@ -163,7 +180,7 @@ struct Launchers {
                               uint32_t policy_bfs, uint32_t max_ev) {
         if (n == 0) return cudaSuccess;
         constexpr int K = kInsertKPT;
-        const int grid = grid_for(n, L.block, K, L.max_grid);
+        const int grid = L.full_grid ? full_grid_for(n, L.block, K) : grid_for(n, L.block, K, L.max_grid);
         { k_insert<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
                                                        aligned(keys, key_vec_align<C, K>()), aligned(out, K),
                                                        policy_bfs, max_ev); CF_COUNT_LAUNCH(); }

@@ -204,7 +204,13 @@ typedef enum cf_option {
      * tables above 4 GiB get larger regions. */
     CF_OPT_REGION_BYTES = 7,
     /* Read-only: number of regions of the region-staged path. */
-    CF_OPT_REGION_COUNT = 8
+    CF_OPT_REGION_COUNT = 8,
+    /* Random-probe lookups: keys per thread (1, 2 or 4; 0 = default). */
+    CF_OPT_LOOKUP_KPT = 9,
+    /* Random-probe kernels (lookups, deletes, inserts): 0 = one tile of keys
+     * per CTA, the grid sized by the batch (default: measured fastest on B200);
+     * 1 = a persistent grid of one wave of CTAs striding over the batch. */
+    CF_OPT_PERSISTENT = 10
 } cf_option;
 
 /* Execution paths (CF_OPT_STAGING).  All give the same per-key results. */

@@ -54,3 +54,18 @@ def test_positive_sample_without_replacement():
     pos = set(fill.tolist())
     qp = [x for x in query.tolist() if x in pos]
     assert len(qp) == 20000 == len(set(qp))
+
+
+def test_segmented_splitmix64_matches_oracle(orc):
+    """The batched form's key generator: segment i is splitmix64(seed_i) from output first_i."""
+    import numpy as np
+    import torch
+
+    import bench
+
+    seeds = np.array([0, 7, 4095, 1 << 40], np.int64)
+    counts = np.array([5, 0, 17, 3], np.int64)
+    first = np.array([0, 0, 2, 1], np.int64)
+    got = bench.splitmix64_segments(seeds, counts, first, torch.device("cpu")).numpy().view(np.uint64)
+    want = np.concatenate([orc.splitmix64(int(s), int(c) + int(f))[int(f):] for s, c, f in zip(seeds, counts, first)])
+    assert np.array_equal(got, want)
