@@ -37,6 +37,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
@@ -752,6 +754,53 @@ def run_batched(args) -> dict:
     return res
 
 
+# ------------------------------------------------------------- served form
+
+
+def run_served(args) -> dict:
+    """Served form: 256 tenant filters (capacities log-uniform 2^16..2^26
+    slots, 8- or 16-bit tags) admitted under a 120 GB HBM budget; Poisson
+    request arrivals at each offered load; 60/30/10 lookup/insert/delete;
+    request sizes lognormal (median 16K keys, clipped 1K..1M).  Continuous
+    batching over filter sets against a FIFO of plain per-request API calls."""
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    import cuckoo_b200.serving as srv
+
+    torch.cuda.set_device(0)
+    tenants = srv.make_tenants(args.tenants, seed=args.batched_seed)
+    loads = [float(x) for x in args.loads.split(",")]
+    out = {"form": "served", "metric": "p50/p99 request latency and sustained Mkeys/s vs offered load",
+           "unit": "ms / Mkeys/s", "n_gpus": 1, "dtype": "u64",
+           "data": "synthetic: per-tenant splitmix64 streams, Poisson arrivals",
+           "config": {"workload": "served: 256 tenants, capacities log-uniform 2^16..2^26 slots, 8/16-bit tags, "
+                                  "16-slot buckets; 60/30/10 lookup/insert/delete; sizes lognormal(median 16384, "
+                                  "sigma 1) clipped 1K..1M", "tenants": args.tenants,
+                      "hbm_budget_gb": args.budget_gb, "duration_s_per_load": args.duration}, "loads": []}
+    for i, load in enumerate(loads):
+        trace = srv.make_trace(tenants, load * 1e6, args.duration, seed=100 + i)
+        server = srv.Server(cfb, tenants, hbm_budget_bytes=int(args.budget_gb * 1e9), max_wave_keys=1 << 24)
+        try:
+            served = server.run(trace)
+            waves, launches = server.waves, server.launches
+            admitted = len(server.admitted)
+        finally:
+            server.close()
+        st = srv.latency_stats(served)
+        import copy
+
+        plain = srv.serve_plain(cfb, tenants, [copy.copy(r) for r in trace])
+        sp = srv.latency_stats(plain)
+        same = all(np.array_equal(a.result, b.result) for a, b in zip(served, plain))
+        out["loads"].append({"offered_mkeys_s": load, "requests": st["requests"], "keys": st["keys"],
+                             "served": {**st, "waves": waves, "kernel_launches": launches, "admitted": admitted},
+                             "plain_fifo": sp, "results_identical": same})
+    return out
+
+
 # ------------------------------------------------------------ reference arm
 
 
@@ -855,8 +904,13 @@ def main() -> None:
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--cpu-scale", type=int, default=27, help="log2 slots of the CPU-baseline sample")
     ap.add_argument("--ref-scale", type=int, default=25, help="log2 slots of each reference-arm CPU step")
-    ap.add_argument("--form", choices=("plain", "batched"), default="plain",
-                    help="batched: the filter-set form over 4096 uneven filters (its own JSON line)")
+    ap.add_argument("--form", choices=("plain", "batched", "served"), default="plain",
+                    help="batched: the filter-set form over 4096 uneven filters; served: the multi-tenant "
+                         "continuous-batching form (each its own JSON line)")
+    ap.add_argument("--tenants", type=int, default=256)
+    ap.add_argument("--loads", default="10,50,100,200", help="offered loads of the served form, Mkeys/s")
+    ap.add_argument("--duration", type=float, default=0.5, help="seconds of arrivals per offered load")
+    ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--filters", type=int, default=4096)
     ap.add_argument("--batched-seed", type=int, default=1)
     args = ap.parse_args()
@@ -865,6 +919,8 @@ def main() -> None:
     w = WORKLOADS[args.workload]
     if args.form == "batched":
         res = run_batched(args)
+    elif args.form == "served":
+        res = run_served(args)
     else:
         res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
     if res is not None:
