@@ -801,6 +801,133 @@ def run_served(args) -> dict:
     return out
 
 
+# ------------------------------------------------------------ k-mer workload
+
+
+def markov_dna(n_bases: int, chains: int, seed: int, device):
+    """A DNA string (uint8 bases A=0 C=1 G=2 T=3) from an order-3 Markov chain
+    whose 64 transition rows are seeded Dirichlet(1) draws (Exp(1) normalised).
+    `chains` independent chains run in parallel and are concatenated."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    rows = -torch.log(torch.rand(64, 4, generator=g, device=device, dtype=torch.float64))  # Exp(1)
+    rows = rows / rows.sum(1, keepdim=True)
+    cum = torch.cumsum(rows, 1)[:, :3].float()  # 3 thresholds per context
+    steps = n_bases // chains
+    seq = torch.empty(chains, steps, dtype=torch.uint8, device=device)
+    state = torch.randint(0, 64, (chains,), generator=g, device=device)
+    for t in range(steps):
+        u = torch.rand(chains, generator=g, device=device)
+        c = cum[state]
+        base = (u > c[:, 0]).to(torch.int64) + (u > c[:, 1]) + (u > c[:, 2])
+        seq[:, t] = base.to(torch.uint8)
+        state = ((state << 2) | base) & 63
+    return seq.reshape(-1)
+
+
+def mutate(bases, rate: float, seed: int):
+    """Copy of `bases` with each base substituted by a different one with probability `rate`."""
+    import torch
+
+    g = torch.Generator(device=bases.device)
+    g.manual_seed(seed)
+    hit = torch.rand(bases.numel(), generator=g, device=bases.device) < rate
+    shift = torch.randint(1, 4, (bases.numel(),), generator=g, device=bases.device, dtype=torch.uint8)
+    return torch.where(hit, (bases + shift) % 4, bases)
+
+
+def canonical_kmers(bases, k: int = 31):
+    """Canonical k-mers (min of the 2-bit MSB-first forward encoding and its
+    reverse complement) of every window, as int64."""
+    import torch
+
+    n = bases.numel() - k + 1
+    b = bases.to(torch.int64)
+    fwd = torch.zeros(n, dtype=torch.int64, device=bases.device)
+    rc = torch.zeros(n, dtype=torch.int64, device=bases.device)
+    for j in range(k):
+        w = b[j:j + n]
+        fwd |= w << (2 * (k - 1 - j))
+        rc |= (3 - w) << (2 * j)
+    return torch.minimum(fwd, rc)
+
+
+def run_kmer(args) -> dict:
+    """Synthetic k-mer workload: a 2^28-base order-3 Markov DNA string, its
+    distinct canonical 31-mers inserted in 20 equal steps up to 0.95 load
+    (or as far as the distinct k-mers go), insert Gkeys/s and eviction-chain
+    histogram per step; then lookups of the 31-mers of a copy with 1 % random
+    substitutions."""
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    n_bases = 1 << args.kmer_bases_log2
+    t0 = time.perf_counter()
+    dna = markov_dna(n_bases, 1 << 14, args.batched_seed, dev)
+    kmers = torch.unique(canonical_kmers(dna))
+    g = torch.Generator(device=dev)
+    g.manual_seed(args.batched_seed + 1)
+    kmers = kmers[torch.randperm(kmers.numel(), generator=g, device=dev)]
+    queries = canonical_kmers(mutate(dna, 0.01, args.batched_seed + 2))
+    gen_s = time.perf_counter() - t0
+    out = {"form": "kmer", "metric": "insert Gkeys/s per load step; lookup Gkeys/s and hit rate",
+           "unit": "Gkeys/s", "n_gpus": 1, "dtype": "u64",
+           "data": f"synthetic: 2^{args.kmer_bases_log2}-base order-3 Markov DNA (Dirichlet(1) rows), canonical "
+                   "31-mers 2-bit MSB-first, deduplicated; queries from a 1%-substituted copy",
+           "config": {"workload": "kmer", "bases": n_bases, "distinct_kmers": int(kmers.numel()),
+                      "query_windows": int(queries.numel()), "generation_s": gen_s}, "filters": []}
+    stream = torch.cuda.current_stream()
+    for cap_log2, bits in ((26, 8), (30, 16)):
+        cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=bits, bucketSize=16, maxEvictions=500,
+                               evictionPolicy=cfb.EvictionPolicy.BFS)
+        f = cfb.CuckooFilter(cfg, 1 << cap_log2)
+        f.setOption(cfb.OPT_CHAIN_HISTOGRAM, 1)
+        target = int(0.95 * f.capacity())
+        n_ins = min(target, kmers.numel())
+        per = n_ins // 20
+        steps = []
+        prev_hist = np.zeros(10, np.uint64)
+        for st_i in range(20):
+            a = st_i * per
+            b = n_ins if st_i == 19 else a + per
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            occ = f.insertMany(kmers[a:b], stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            hist = f.chainHistogram()
+            stt = f.stats()
+            steps.append({"step": st_i + 1, "keys": b - a, "load": occ / f.capacity(), "ms": ms,
+                          "insert_gkeys_s": (b - a) / ms / 1e6, "failed_total": stt["failed"],
+                          "chain_histogram": (hist - prev_hist).tolist()})
+            prev_hist = hist
+        q_out = torch.empty(queries.numel(), dtype=torch.bool, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f.containsManyAsync(queries, q_out, stream=stream)  # warm-up
+        e0.record(stream)
+        f.containsManyAsync(queries, q_out, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out["filters"].append({
+            "capacity_slots": f.capacity(), "bits_per_tag": bits, "table_bytes": f.sizeInBytes(),
+            "l2_resident": f.sizeInBytes() <= (126 << 20), "inserted": n_ins, "final_load": f.loadFactor(),
+            "reached_target_load": n_ins == target,
+            "chain_bins": "0 moves, 1, 2-3, 4-7, 8-15, 16-31, 32-63, 64-127, 128-255, >=256",
+            "steps": steps, "lookup": {"keys": int(queries.numel()), "ms": ms,
+                                       "gkeys_s": queries.numel() / ms / 1e6,
+                                       "hit_rate": float(q_out.float().mean().item())}})
+        f.close()
+    return out
+
+
 # ------------------------------------------------------------ reference arm
 
 
@@ -904,7 +1031,8 @@ def main() -> None:
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--cpu-scale", type=int, default=27, help="log2 slots of the CPU-baseline sample")
     ap.add_argument("--ref-scale", type=int, default=25, help="log2 slots of each reference-arm CPU step")
-    ap.add_argument("--form", choices=("plain", "batched", "served"), default="plain",
+    ap.add_argument("--kmer-bases-log2", type=int, default=28)
+    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer"), default="plain",
                     help="batched: the filter-set form over 4096 uneven filters; served: the multi-tenant "
                          "continuous-batching form (each its own JSON line)")
     ap.add_argument("--tenants", type=int, default=256)
@@ -921,6 +1049,8 @@ def main() -> None:
         res = run_batched(args)
     elif args.form == "served":
         res = run_served(args)
+    elif args.form == "kmer":
+        res = run_kmer(args)
     else:
         res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
     if res is not None:

@@ -52,6 +52,7 @@ OPT_REGION_BYTES = 7
 OPT_REGION_COUNT = 8
 OPT_LOOKUP_KPT = 9
 OPT_PERSISTENT = 10
+OPT_CHAIN_HISTOGRAM = 11
 NEVER = (1 << 64) - 1
 
 # cf_staging values (OPT_STAGING)
@@ -98,6 +99,7 @@ def library() -> C.CDLL:
     sig = {
         "cf_abi_version": ([], i32),
         "cf_launch_count": ([], u64),
+        "cf_get_chain_histogram": ([vp, vp], i32),
         "cf_last_error": ([], C.c_char_p),
         "cf_status_string": ([i32], C.c_char_p),
         "cf_config_supported": ([C.POINTER(_Config)], i32),
@@ -364,6 +366,14 @@ class CuckooFilter:
         s = _Stats()
         _check(library().cf_get_stats(self._h, C.byref(s)))
         return {name: int(getattr(s, name)) for name, _ in _Stats._fields_}
+
+    def chainHistogram(self):
+        """Eviction-chain-length histogram (CF_CHAIN_BINS bins; see cuckoo_b200.h)."""
+        import numpy as np
+
+        out = np.zeros(10, np.uint64)
+        _check(library().cf_get_chain_histogram(self._h, out.ctypes.data))
+        return out
 
     def evictionCount(self) -> int:
         return self.stats()["evictions"]

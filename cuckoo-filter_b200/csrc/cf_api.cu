@@ -49,6 +49,7 @@ struct cf_filter {
     uint64_t rg_bytes;      // CF_OPT_REGION_BYTES (0 = kRgRegionBytes)
     uint32_t lookup_kpt;    // CF_OPT_LOOKUP_KPT (0 = default)
     uint32_t persistent;    // CF_OPT_PERSISTENT (0 = one tile per CTA, 1 = persistent grid)
+    uint32_t chain_hist;    // CF_OPT_CHAIN_HISTOGRAM
 };
 
 namespace {
@@ -129,7 +130,9 @@ uint64_t num_buckets_for(uint64_t capacity, uint32_t bucket_size) {
     return n + 1;
 }
 
-DevTable dev(const cf_filter* f) { return DevTable{f->d_table, f->num_buckets - 1, f->d_ctr}; }
+DevTable dev(const cf_filter* f) {
+    return DevTable{f->d_table, f->num_buckets - 1, f->d_ctr, f->chain_hist ? f->d_ctr + CTR_HIST0 : nullptr};
+}
 
 LaunchCfg launch(const cf_filter* f, int kid, void* stream) {
     LaunchCfg L{static_cast<cudaStream_t>(stream), f->block, f->max_grid[kid]};
@@ -619,6 +622,16 @@ int cf_get_stats(cf_filter* f, cf_stats* out) {
     return CF_OK;
 }
 
+int cf_get_chain_histogram(cf_filter* f, uint64_t* bins) {
+    if (int s = check_filter(f)) return s;
+    if (!bins) return fail(CF_ERR_INVALID, "bins is NULL");
+    DeviceGuard g(f->device);
+    unsigned long long h[kChainBins];
+    CF_CUDA(cudaMemcpy(h, f->d_ctr + CTR_HIST0, sizeof(h), cudaMemcpyDeviceToHost), "histogram read");
+    for (int i = 0; i < kChainBins; ++i) bins[i] = h[i];
+    return CF_OK;
+}
+
 int cf_reset_stats(cf_filter* f) {
     if (int s = check_filter(f)) return s;
     DeviceGuard g(f->device);
@@ -677,6 +690,10 @@ int cf_set_option(cf_filter* f, int option, uint64_t value) {
             if (value > 1) return fail(CF_ERR_INVALID, "persistent must be 0 or 1");
             f->persistent = static_cast<uint32_t>(value);
             return CF_OK;
+        case CF_OPT_CHAIN_HISTOGRAM:
+            if (value > 1) return fail(CF_ERR_INVALID, "chain histogram must be 0 or 1");
+            f->chain_hist = static_cast<uint32_t>(value);
+            return CF_OK;
         case CF_OPT_REGION_BYTES:
             if (value & (value - 1)) return fail(CF_ERR_INVALID, "region bytes must be 0 or a power of two");
             f->rg_bytes = value;
@@ -701,6 +718,7 @@ int cf_get_option(cf_filter* f, int option, uint64_t* value) {
         case CF_OPT_REGION_COUNT: *value = f->rgeom.nreg; return CF_OK;
         case CF_OPT_LOOKUP_KPT: *value = f->lookup_kpt; return CF_OK;
         case CF_OPT_PERSISTENT: *value = f->persistent; return CF_OK;
+        case CF_OPT_CHAIN_HISTOGRAM: *value = f->chain_hist; return CF_OK;
         default: return fail(CF_ERR_INVALID, "unknown option %d", option);
     }
 }

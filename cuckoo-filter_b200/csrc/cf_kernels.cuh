@@ -48,8 +48,11 @@ enum Counter : int {
     CTR_ERROR = 7,
     CTR_REMOVED = 8,
     CTR_DUP = 9,
-    CTR_COUNT = 16
+    CTR_HIST0 = 16,  // eviction-chain-length histogram, kChainBins counters
+    CTR_COUNT = 32
 };
+// Chain-length bins: 0 evictions (a slot freed up), 1, 2-3, 4-7, ..., >= 256.
+constexpr int kChainBins = 10;
 constexpr uint64_t ERR_CAS_LIMIT = 1;   // a compare-and-swap retry bound was hit
 constexpr uint64_t ERR_WAIT_LIMIT = 2;  // a bulk copy did not complete within its poll bound
 
@@ -57,7 +60,15 @@ struct DevTable {
     uint8_t* buckets;
     uint64_t nb_mask;
     unsigned long long* ctr;
+    unsigned long long* hist = nullptr;  // chain-length histogram (kChainBins), or null when not recorded
 };
+
+// Records the eviction chain of one stored key (L slot exchanges).
+__device__ __forceinline__ void record_chain(const DevTable& t, uint32_t L) {
+    if (!t.hist) return;
+    const int bin = L == 0 ? 0 : (32 - __clz(L)) < kChainBins - 1 ? (32 - __clz(L)) : kChainBins - 1;
+    atomicAdd(&t.hist[bin], 1ull);
+}
 
 template <class C>
 __device__ __forceinline__ uint64_t* bucket_words(const DevTable& t, uint64_t b) {
@@ -465,8 +476,11 @@ __device__ __noinline__ bool evict_key(DevTable t, uint64_t key, uint32_t policy
     const uint64_t i2 = alt_bucket<C>(i1, fp, t.nb_mask);
     const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
     const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
-    return policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
-                      : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+    const uint32_t before = st.evictions;
+    const bool ok = policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
+                               : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+    if (ok) record_chain(t, st.evictions - before);
+    return ok;
 }
 
 // Inclusive prefix sum across the warp.

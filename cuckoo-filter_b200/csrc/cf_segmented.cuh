@@ -840,6 +840,7 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
         if (outcome == 1 || outcome == 2) {
             ++n_ok;
             if (outcome == 2) ++n_ev;
+            record_chain(t, outcome == 2 ? 1u : 0u);
             if (bitmap) atomicOr(&bitmap[pay[idx] >> 5], 1u << (pay[idx] & 31));
         }
         const uint32_t push = __ballot_sync(0xFFFFFFFFu, outcome == 3);
@@ -884,8 +885,10 @@ __global__ void __launch_bounds__(256) k_evict_list(DevTable t, const uint64_t* 
         const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
         const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
         ++n_evk;
+        const uint32_t before = st.evictions;
         const bool ok = policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
                                    : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+        if (ok) record_chain(t, st.evictions - before);
         if (ok) {
             if (bitmap) {
                 const uint32_t p = pay[i];

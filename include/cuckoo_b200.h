@@ -210,8 +210,20 @@ typedef enum cf_option {
     /* Random-probe kernels (lookups, deletes, inserts): 0 = one tile of keys
      * per CTA, the grid sized by the batch (default: measured fastest on B200);
      * 1 = a persistent grid of one wave of CTAs striding over the batch. */
-    CF_OPT_PERSISTENT = 10
+    CF_OPT_PERSISTENT = 10,
+    /* 1 = record the eviction-chain-length histogram of inserts
+     * (cf_get_chain_histogram); 0 = off (default; one atomic per evicting
+     * insert when on). */
+    CF_OPT_CHAIN_HISTOGRAM = 11
 } cf_option;
+
+/* Eviction-chain-length histogram since creation, cf_clear or cf_reset_stats,
+ * recorded while CF_OPT_CHAIN_HISTOGRAM is on: bins[0] = inserts that needed
+ * eviction but found a free slot without moving a tag, bins[b] for b >= 1 =
+ * stored inserts whose chain moved L tags with 2^(b-1) <= L < 2^b (the last
+ * bin holds every L >= 256).  Failed inserts are counted in cf_stats.failed. */
+#define CF_CHAIN_BINS 10
+int cf_get_chain_histogram(cf_filter* f, uint64_t* bins);
 
 /* Execution paths (CF_OPT_STAGING).  All give the same per-key results. */
 typedef enum cf_staging {

@@ -69,3 +69,36 @@ def test_segmented_splitmix64_matches_oracle(orc):
     got = bench.splitmix64_segments(seeds, counts, first, torch.device("cpu")).numpy().view(np.uint64)
     want = np.concatenate([orc.splitmix64(int(s), int(c) + int(f))[int(f):] for s, c, f in zip(seeds, counts, first)])
     assert np.array_equal(got, want)
+
+
+def test_canonical_kmers_match_a_direct_encoding():
+    """2-bit MSB-first encoding (A0 C1 G2 T3), canonical = min(forward, reverse complement)."""
+    import numpy as np
+    import torch
+
+    import bench
+
+    rng = np.random.default_rng(0)
+    b = rng.integers(0, 4, 200).astype(np.uint8)
+    got = bench.canonical_kmers(torch.from_numpy(b), k=31).numpy()
+    for i in (0, 1, 77, 169):
+        w = b[i:i + 31]
+        fwd = sum(int(x) << (2 * (30 - j)) for j, x in enumerate(w))
+        rc = sum(int(3 - x) << (2 * (30 - j)) for j, x in enumerate(w[::-1]))
+        assert got[i] == min(fwd, rc)
+    # a window and its reverse complement share the canonical k-mer
+    rcs = (3 - b[::-1]).copy()
+    got_rc = bench.canonical_kmers(torch.from_numpy(rcs), k=31).numpy()
+    assert set(got.tolist()) == set(got_rc.tolist())
+
+
+def test_markov_dna_and_mutation_cpu():
+    import torch
+
+    import bench
+
+    dna = bench.markov_dna(1 << 12, 16, seed=1, device=torch.device("cpu"))
+    assert dna.numel() == 4096 and int(dna.max()) <= 3
+    m = bench.mutate(dna, 0.01, seed=2)
+    diff = (m != dna).float().mean().item()
+    assert 0.0 < diff < 0.03

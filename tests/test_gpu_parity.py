@@ -375,3 +375,24 @@ def test_clear_and_counters(cfb, orc):
     assert f.occupiedSlots() == 0 and f.countOccupiedSlots() == 0
     assert not host_u8(f.containsMany(keys)).any()
     assert f.stats()["primary"] == 0
+
+
+@pytest.mark.parametrize("staging", ["random", "segment", "region"])
+@pytest.mark.parametrize("policy", [0, 1])
+def test_chain_histogram_accounts_for_every_evicting_insert(cfb, orc, staging, policy):
+    f, o = make(cfb, orc, 8, 16, 16, policy, 500, 1 << 18, staging)
+    f.setOption(cfb.OPT_CHAIN_HISTOGRAM, 1)
+    keys = orc.splitmix64(21, int(0.97 * f.capacity()))
+    if staging == "segment":
+        f.insertManySorted(dev(keys))
+    else:
+        f.insertMany(dev(keys))
+    st = f.stats()
+    hist = f.chainHistogram()
+    assert st["evicted_inserts"] > 0
+    assert int(hist.sum()) == st["evicted_inserts"] - st["failed"], (hist.tolist(), st)
+    # chains move at most maxEvictions tags; BFS resolves most with one move
+    if policy == 0:
+        assert hist[1] > hist[2:].sum()
+    f.resetEvictionCount()
+    assert int(f.chainHistogram().sum()) == 0
