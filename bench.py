@@ -928,6 +928,65 @@ def run_kmer(args) -> dict:
     return out
 
 
+# ------------------------------------------------------------- config grid
+
+
+def run_grid(args) -> dict:
+    """The large filter across tag/bucket geometries, eviction policies and
+    insert paths: 2^31 slots, {8/16, 16/16, 32/8} x {BFS, DFS} x {insertMany,
+    insertManySorted}; fill to 0.95, 2^28 lookups (50 % positive), 2^26 deletes."""
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    base = dict(WORKLOADS["large"])
+    fill, query, dele, _ = make_inputs(base, dev)
+    q_out = torch.empty(query.numel(), dtype=torch.bool, device=dev)
+    stream = torch.cuda.current_stream()
+    rows = []
+    for bits, bs in ((8, 16), (16, 16), (32, 8)):
+        for pol in ("BFS", "DFS"):
+            cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=bits, bucketSize=bs, maxEvictions=500,
+                                   evictionPolicy=cfb.EvictionPolicy[pol])
+            f = cfb.CuckooFilter(cfg, base["capacity"])
+            f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
+            for path in ("insertMany", "insertManySorted"):
+                res = {}
+                for k in range(2):  # the first pass warms the workspace and the caches
+                    f.clear(stream)
+                    f.resetEvictionCount()
+                    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                    e[0].record(stream)
+                    if path == "insertMany":
+                        f.insertManyAsync(fill, stream=stream)
+                    else:
+                        f.insertManySorted(fill, stream=stream)
+                    e[1].record(stream)
+                    f.containsManyAsync(query, q_out, stream=stream)
+                    e[2].record(stream)
+                    f.deleteManyAsync(dele, stream=stream)
+                    e[3].record(stream)
+                    torch.cuda.synchronize()
+                    st = f.stats()
+                    res = {"geometry": f"{bits}/{bs}", "eviction": pol, "insert_path": path,
+                           "table_bytes": f.sizeInBytes(),
+                           "insert_gkeys_s": fill.numel() / e[0].elapsed_time(e[1]) / 1e6,
+                           "lookup_gkeys_s": query.numel() / e[1].elapsed_time(e[2]) / 1e6,
+                           "delete_gkeys_s": dele.numel() / e[2].elapsed_time(e[3]) / 1e6,
+                           "failed": st["failed"], "lost": st["lost"], "evictions": st["evictions"],
+                           "lookup_hits": int(q_out.sum().item())}
+                rows.append(res)
+                print(json.dumps(res), file=sys.stderr, flush=True)
+            f.close()
+    return {"form": "grid", "metric": "Gkeys/s per op across geometries, eviction policies and insert paths",
+            "unit": "Gkeys/s", "n_gpus": 1, "dtype": "u64", "data": "synthetic: splitmix64 keys (large workload)",
+            "config": {"workload": "large filter grid: 2^31 slots; fill 0.95 (2 040 109 465 keys), 2^28 lookups "
+                                   "50% positive, 2^26 deletes"}, "rows": rows}
+
+
 # ------------------------------------------------------------ reference arm
 
 
@@ -1032,7 +1091,7 @@ def main() -> None:
     ap.add_argument("--cpu-scale", type=int, default=27, help="log2 slots of the CPU-baseline sample")
     ap.add_argument("--ref-scale", type=int, default=25, help="log2 slots of each reference-arm CPU step")
     ap.add_argument("--kmer-bases-log2", type=int, default=28)
-    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer"), default="plain",
+    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid"), default="plain",
                     help="batched: the filter-set form over 4096 uneven filters; served: the multi-tenant "
                          "continuous-batching form (each its own JSON line)")
     ap.add_argument("--tenants", type=int, default=256)
@@ -1051,6 +1110,8 @@ def main() -> None:
         res = run_served(args)
     elif args.form == "kmer":
         res = run_kmer(args)
+    elif args.form == "grid":
+        res = run_grid(args)
     else:
         res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
     if res is not None:
