@@ -223,7 +223,7 @@ int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     CF_CUDA(rs_scatter_grid<1>(f->sms, &rs_grid[1]), "radix launch setup");
     CF_CUDA(rs_scatter_grid<2>(f->sms, &rs_grid[2]), "radix launch setup");
     const int rg_grid = f->sms * 4;
-    const int grid = std::max(std::max(rs_grid[0], std::max(rs_grid[1], rs_grid[2])),
+    const int grid = std::max(std::max(rs_grid[0], std::max(rs_grid[1], rs_grid[2])) * kRsHistSub,
                               (rg_grid * static_cast<int>(kRgMaxRegions) + kRadix - 1) / kRadix);
     const uint64_t fixed = ws_need(f, 0, grid, payload) + 4096;
     uint64_t cap = n;
@@ -828,7 +828,7 @@ constexpr uint64_t na_al(uint64_t x) { return (x + 255) & ~255ull; }
 constexpr uint64_t kNaEnt = na_al(kNoAllocMaxKeys * 8);
 constexpr uint64_t kNaPay = na_al(kNoAllocMaxKeys * 4);
 constexpr uint64_t kNaBitmap = na_al((2 * kNoAllocMaxKeys + 31) / 32 * 4);
-constexpr uint64_t kNaHist = na_al(static_cast<uint64_t>(kRadix) * kNoAllocMaxGrid * 4);
+constexpr uint64_t kNaHist = na_al(static_cast<uint64_t>(kRadix) * kNoAllocMaxGrid * kRsHistSub * 4);
 constexpr uint64_t kNaStart = na_al((kNoAllocMaxSegments + 1) * 4);
 constexpr uint64_t kNaCnt = 256;
 constexpr uint64_t kNoAllocScratchBytes = 2 * kNaEnt + 2 * kNaPay + kNaBitmap + kNaHist + kNaStart + kNaCnt;

@@ -124,13 +124,15 @@ int blocks_per_sm(K kernel, int threads, size_t smem) {
     return bps;
 }
 
-// CTAs in one wave of the radix scatter for payload mode PAY.
+// CTAs of the radix scatter for payload mode PAY: one wave, at most two CTAs
+// per SM (on B200 a 2^31-entry pass took 8.5 ms at two CTAs per SM against
+// 9.6 ms at the three that fit).
 template <int PAY>
 cudaError_t rs_scatter_grid(int sms, int* grid) {
     cudaError_t e = ensure_smem_attr<k_rs_scatter<PAY>>(rs_scatter_smem<PAY>());
     if (e != cudaSuccess) return e;
     static const int bps = blocks_per_sm(k_rs_scatter<PAY>, kRsThreads, rs_scatter_smem<PAY>());
-    *grid = sms * bps;
+    *grid = sms * (bps < 2 ? bps : 2);
     return cudaSuccess;
 }
 
@@ -225,21 +227,22 @@ struct Launchers {
                                int shift, int order_bits, int dst, const SegWork& w, cudaStream_t s, int lo_bits) {
         const int pay = !payload ? 0 : keys_mode ? 1 : 2;
         const int grid = w.rs_grid[pay];
-        const uint32_t hist_n = static_cast<uint32_t>(kRadix) * static_cast<uint32_t>(grid);
+        const int hgrid = grid * kRsHistSub;
+        const uint32_t hist_n = static_cast<uint32_t>(kRadix) * static_cast<uint32_t>(hgrid);
         const uint64_t* ent_src = keys_mode ? w.ent[1] : w.ent[from];
         const void* hsrc = keys_mode ? src : static_cast<const void*>(ent_src);
         uint64_t* hout = keys_mode ? w.ent[1] : nullptr;
         if (keys_mode && lo_bits >= 0)
-            { k_rs_hist<C, true, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
+            { k_rs_hist<C, true, true><<<hgrid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
                                                                      lo_bits, w.start); CF_COUNT_LAUNCH(); }
         else if (keys_mode)
-            { k_rs_hist<C, true, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
+            { k_rs_hist<C, true, false><<<hgrid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist, hout,
                                                                       0, nullptr); CF_COUNT_LAUNCH(); }
         else if (lo_bits >= 0)
-            { k_rs_hist<C, false, true><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
+            { k_rs_hist<C, false, true><<<hgrid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
                                                                       nullptr, lo_bits, w.start); CF_COUNT_LAUNCH(); }
         else
-            { k_rs_hist<C, false, false><<<grid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
+            { k_rs_hist<C, false, false><<<hgrid, kRsHistThreads, 0, s>>>(hsrc, t.nb_mask, n, nullptr, shift, w.hist,
                                                                        nullptr, 0, nullptr); CF_COUNT_LAUNCH(); }
         { k_scan_u32<<<1, 1024, 0, s>>>(w.hist, hist_n); CF_COUNT_LAUNCH(); }
         unsigned long long* err = t.ctr + CTR_ERROR;
@@ -289,10 +292,12 @@ struct Launchers {
         // the insert kernel stages a slot mask per bucket beside the segment
         constexpr int kMaxSmem = OP == SEG_INSERT ? kSegBytes + (kSegBytes / C::bucket_bytes) * sizeof(SlotMask<C>)
                                                   : kSegBytes;
-        constexpr auto kern = OP == SEG_INSERT ? k_seg_insert<C> : k_seg<C, OP>;
+        constexpr auto kern = OP == SEG_INSERT ? k_seg_insert<C, false> : k_seg<C, OP>;
+        constexpr auto kern_pay = OP == SEG_INSERT ? k_seg_insert<C, true> : k_seg<C, OP>;
         const int smem = static_cast<int>(OP == SEG_INSERT ? seg_insert_smem<C>(g.sb_log2)
                                                            : (1ull << g.sb_log2) * C::bucket_bytes);
         cudaError_t e = ensure_smem_attr<kern>(kMaxSmem);
+        if (e == cudaSuccess) e = ensure_smem_attr<kern_pay>(kMaxSmem);
         if (e != cudaSuccess) return e;
         if (!have_start) {
             const uint64_t bthreads = n / 8 + 1;  // 8 positions per thread
@@ -302,9 +307,11 @@ struct Launchers {
         const int other = 1 - buf;
         // one CTA per segment (measured faster on B200 than one wave of CTAs
         // striding over the segments)
-        { kern<<<static_cast<int>(g.nseg < 0x7FFFFFFFull ? g.nseg : 0x7FFFFFFFull), kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start, g.nseg,
-                                                    g.sb_log2, round, w.ent[other], payload ? w.pay[other] : nullptr,
-                                                    &w.cnt[round - 1], payload ? w.bitmap : nullptr); CF_COUNT_LAUNCH(); }
+        const int grid = static_cast<int>(g.nseg < 0x7FFFFFFFull ? g.nseg : 0x7FFFFFFFull);
+        { (payload ? kern_pay : kern)<<<grid, kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr,
+                                                                     w.start, g.nseg, g.sb_log2, round, w.ent[other],
+                                                                     payload ? w.pay[other] : nullptr, &w.cnt[round - 1],
+                                                                     payload ? w.bitmap : nullptr); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
 

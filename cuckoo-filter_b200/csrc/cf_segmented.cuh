@@ -35,9 +35,12 @@ constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kRsIPT = 8;
+constexpr int kRsIPT = 16;
 constexpr int kRsTile = kRsThreads * kRsIPT;
 constexpr int kRsHistThreads = 512;
+// Histogram CTAs per scatter CTA: each counts one part of the scatter CTA's
+// chunk, so the histogram pass runs on three times the scatter's grid.
+constexpr int kRsHistSub = 3;
 static_assert(kRsThreads == kRadix, "the scatter's per-digit phases give one thread per digit");
 constexpr int kSegBytes = 65536;
 constexpr int kSegThreads = 256;
@@ -65,12 +68,14 @@ __device__ __forceinline__ uint64_t item_count(uint64_t n, const unsigned long l
     return n_dev ? static_cast<uint64_t>(*n_dev) : n;
 }
 
-__device__ __forceinline__ uint64_t chunk_of(uint64_t n) {
-    const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
+__device__ __forceinline__ uint64_t chunk_of(uint64_t n, uint32_t parts) {
+    const uint64_t per = (n + parts - 1) / parts;
     return (per + kRsTile - 1) / kRsTile * kRsTile;
 }
 
-// Per-CTA digit histogram of its contiguous chunk: hist[digit * grid + cta].
+// Digit histogram of each scatter CTA's contiguous chunk, counted by
+// kRsHistSub CTAs per chunk: hist[(digit * scatter grid + cta) * kRsHistSub +
+// part], so one scan gives every scatter CTA its start per digit.
 // KEYS: items are keys, hashed here into packed entries that are also written
 // to `ent_out` (so later passes never hash again); otherwise packed entries.
 // SEGS (last pass of a sort whose earlier passes ordered the items by the
@@ -91,9 +96,13 @@ __global__ void __launch_bounds__(kRsHistThreads, 3)
     }
     __syncthreads();
     const uint64_t m = item_count(n, n_dev);
-    const uint64_t chunk = chunk_of(m);
-    const uint64_t lo = blockIdx.x * chunk;
-    const uint64_t hi = lo + chunk < m ? lo + chunk : m;
+    const uint32_t sgrid = gridDim.x / kRsHistSub, cta = blockIdx.x / kRsHistSub, part = blockIdx.x % kRsHistSub;
+    const uint64_t chunk = chunk_of(m, sgrid);
+    const uint64_t sub = (chunk / kRsHistSub + 31) / 32 * 32;
+    const uint64_t c_hi = static_cast<uint64_t>(cta) * chunk + chunk < m ? static_cast<uint64_t>(cta) * chunk + chunk : m;
+    const uint64_t lo0 = static_cast<uint64_t>(cta) * chunk + part * sub;
+    const uint64_t lo = lo0 < c_hi ? lo0 : c_hi;
+    const uint64_t hi = lo + sub < c_hi && part + 1 < kRsHistSub ? lo + sub : c_hi;
     const uint64_t* ent = static_cast<const uint64_t*>(src);
     const int lo_shift = shift - lo_bits;
     const uint32_t lo_mask = (1u << lo_bits) - 1u;
@@ -146,28 +155,42 @@ __global__ void __launch_bounds__(kRsHistThreads, 3)
     }
     __syncthreads();
     for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
-        hist[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x] = cnt[d];
+        hist[(static_cast<uint64_t>(d) * sgrid + cta) * kRsHistSub + part] = cnt[d];
         if constexpr (SEGS)
             if (run_cnt[d]) atomicAdd(&seg_count[(static_cast<uint32_t>(d) << lo_bits) | cur], run_cnt[d]);
     }
 }
 
 // Exclusive scan of `count` uint32 values in place (one CTA of 1024 threads,
-// four consecutive values per thread per step).
+// sixteen consecutive values per thread per step, read and written as
+// 16-byte vectors when the array is 16-byte aligned).
 static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t count) {
+    constexpr uint32_t V = 16;
     __shared__ uint32_t warp_tot[32];
     __shared__ uint32_t carry;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool vec = (reinterpret_cast<uintptr_t>(v) & 15) == 0;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (uint32_t base = 0; base < count; base += 4096) {
-        const uint32_t i0 = base + threadIdx.x * 4;
-        uint32_t x[4], s = 0;
+    for (uint32_t base = 0; base < count; base += 1024 * V) {
+        const uint32_t i0 = base + threadIdx.x * V;
+        const bool whole = vec && i0 + V <= count;
+        uint32_t x[V], s = 0;
+        if (whole) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            x[j] = i0 + j < count ? v[i0 + j] : 0u;
-            s += x[j];
+            for (uint32_t q = 0; q < V / 4; ++q) {
+                const uint4 u = reinterpret_cast<const uint4*>(v + i0)[q];
+                x[4 * q] = u.x;
+                x[4 * q + 1] = u.y;
+                x[4 * q + 2] = u.z;
+                x[4 * q + 3] = u.w;
+            }
+        } else {
+#pragma unroll
+            for (uint32_t j = 0; j < V; ++j) x[j] = i0 + j < count ? v[i0 + j] : 0u;
         }
+#pragma unroll
+        for (uint32_t j = 0; j < V; ++j) s += x[j];
         const uint32_t incl = warp_inclusive_scan(s);
         if (lane == 31) warp_tot[warp] = incl;
         __syncthreads();
@@ -178,9 +201,19 @@ static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t 
         __syncthreads();
         uint32_t run = carry + warp_tot[warp] + incl - s;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            if (i0 + j < count) v[i0 + j] = run;
-            run += x[j];
+        for (uint32_t j = 0; j < V; ++j) {
+            const uint32_t c = x[j];
+            x[j] = run;
+            run += c;
+        }
+        if (whole) {
+#pragma unroll
+            for (uint32_t q = 0; q < V / 4; ++q)
+                reinterpret_cast<uint4*>(v + i0)[q] = make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (uint32_t j = 0; j < V; ++j)
+                if (i0 + j < count) v[i0 + j] = x[j];
         }
         __syncthreads();
         if (threadIdx.x == 1023) carry = run;
@@ -188,27 +221,29 @@ static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t 
     }
 }
 
-// Shared memory of k_rs_scatter.
+// Shared memory of k_rs_scatter.  Each tile is staged in digit order in the
+// buffer it arrived in, so one tile is in flight while the other is ranked,
+// staged and written out.
 template <int PAY>
 struct RsScatterSmem {
-    uint64_t in[2][kRsTile];                      // bulk-copy double buffer (entries)
-    uint32_t in_pay[2][PAY == 2 ? kRsTile : 4];   // bulk-copy double buffer (payloads)
-    uint64_t stage[kRsTile];                      // the tile in digit order
-    uint32_t stage_pay[PAY ? kRsTile : 1];
-    uint32_t warp_cnt[kRsWarps][kRadix];          // per-warp digit counts, then their warp prefix
+    uint64_t in[2][kRsTile];                      // bulk-copy double buffer (entries), then the staged tile
+    uint32_t in_pay[2][PAY ? kRsTile : 1];        // payloads: bulk-copied (PAY 2), then staged
+    uint32_t cnt[kRadix];                         // digit counts of the tile (ranking by atomics)
+    uint16_t warp_cnt[kRsWarps][kRadix];          // stable ranking: per-warp digit counts, then their warp prefix
     uint32_t running[kRadix];                     // next output position per digit
     uint32_t tot[kRadix];                         // tile count per digit
-    uint32_t tile_off[kRadix];                    // digit offset in the tile, within its group of 32 digits
-    uint32_t grp_off[kRadix / 32];                // offset of each group of 32 digits
+    uint32_t tile_off[kRadix];                    // first staged position of each digit in the tile
+    uint32_t out_base[kRadix];                    // output index of staged position q = out_base[digit] + q (mod 2^32)
+    uint32_t grp_tot[kRadix / 32];                // tile count of each group of 32 digits
     uint64_t bar[2];
 };
 
 // One LSD pass over packed entries: scatter them to dst by digit, using the
-// scanned histogram as the CTA's starting offset per digit.  Full 2048-entry
-// tiles arrive by bulk copy into a double buffer (the copy of tile t+2 is
-// issued as soon as tile t has been read), so the DRAM reads run ahead of the
-// ranking.  Each tile is ranked in shared memory, staged in digit order and
-// written out as contiguous runs.
+// scanned histogram as the CTA's starting offset per digit.  Full 4096-entry tiles
+// arrive by bulk copy into a double buffer (the copy of tile t+2 is issued
+// when tile t has been written out, so tile t+1 is in flight while tile t is
+// worked on).  Each tile is ranked in shared memory (16 entries per thread),
+// staged in digit order in its own buffer and written out as contiguous runs.
 //
 // The sort only has to group entries by segment, so a pass needs to keep the
 // input order only among entries whose lower `lo_bits` segment bits (the
@@ -221,17 +256,17 @@ struct RsScatterSmem {
 // PAY: 0 = no payload, 1 = the payload of entry i is i itself, 2 = payloads
 // read from src_pay.
 template <int PAY>
-__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __restrict__ src,
-                                                           const uint32_t* __restrict__ src_pay, uint64_t n,
-                                                           const unsigned long long* n_dev, int shift, int lo_bits,
-                                                           const uint32_t* offs, uint64_t* __restrict__ dst,
-                                                           uint32_t* __restrict__ dst_pay, unsigned long long* err) {
+__global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __restrict__ src,
+                                                              const uint32_t* __restrict__ src_pay, uint64_t n,
+                                                              const unsigned long long* n_dev, int shift, int lo_bits,
+                                                              const uint32_t* offs, uint64_t* __restrict__ dst,
+                                                              uint32_t* __restrict__ dst_pay, unsigned long long* err) {
     extern __shared__ __align__(128) unsigned char rs_raw[];
     RsScatterSmem<PAY>& sm = *reinterpret_cast<RsScatterSmem<PAY>*>(rs_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint64_t m = item_count(n, n_dev);
-    const uint64_t chunk = chunk_of(m);
+    const uint64_t chunk = chunk_of(m, gridDim.x);
     const uint64_t lo = blockIdx.x * chunk;
     const uint64_t hi = lo + chunk < m ? lo + chunk : m;
     const uint32_t ntile = lo < hi ? static_cast<uint32_t>((hi - lo + kRsTile - 1) / kRsTile) : 0u;
@@ -239,8 +274,9 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
     const int lo_shift = shift - lo_bits;
     const uint64_t lo_mask = (1ull << lo_bits) - 1ull;
     for (int d = tid; d < kRadix; d += blockDim.x) {
-        sm.running[d] = offs[static_cast<uint64_t>(d) * gridDim.x + blockIdx.x];
+        sm.running[d] = offs[(static_cast<uint64_t>(d) * gridDim.x + blockIdx.x) * kRsHistSub];
         sm.tot[d] = 0;
+        sm.cnt[d] = 0;
     }
     for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&sm.warp_cnt[0][0])[i] = 0;
     if (tid == 0) {
@@ -270,8 +306,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
         const bool full = t < nfull;
         const uint32_t count = full ? static_cast<uint32_t>(kRsTile) : static_cast<uint32_t>(hi - tb);
         uint64_t e[kRsIPT];
-        uint32_t p[kRsIPT], rank[kRsIPT], dig[kRsIPT];
-        __syncthreads();  // the previous tile's write-out and counter reset are done
+        uint32_t p[kRsIPT], rank[kRsIPT];
         uint64_t first, last;
         if (full) {
             if (!mbar_wait(&sm.bar[b], (t >> 1) & 1u, kMbarPollLimit)) failed = true;
@@ -303,19 +338,18 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
         // uniform over the CTA
         const bool stable = lo_bits > 0 && ((first >> lo_shift) & lo_mask) != ((last >> lo_shift) & lo_mask);
         if (!stable) {
-            // rank = arrival order within the digit, counted in warp_cnt[0]
+            // rank = arrival order within the digit, counted in cnt
 #pragma unroll
             for (int j = 0; j < kRsIPT; ++j) {
-                const bool v = full || tb + warp * 32 * kRsIPT + j * 32 + lane < hi;
+                const bool v = full || warp * 32 * kRsIPT + j * 32 + lane < count;
                 const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
-                dig[j] = v ? d : static_cast<uint32_t>(kRadix);
-                rank[j] = v ? atomicAdd(&sm.warp_cnt[0][d], 1u) : 0u;
+                rank[j] = v ? atomicAdd(&sm.cnt[d], 1u) : 0u;
             }
         } else {
             // rank = lane order within the warp's row, rows in order, warps in order
 #pragma unroll
             for (int j = 0; j < kRsIPT; ++j) {
-                const bool v = full || tb + warp * 32 * kRsIPT + j * 32 + lane < hi;
+                const bool v = full || warp * 32 * kRsIPT + j * 32 + lane < count;
                 const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
                 uint32_t peers = __ballot_sync(0xFFFFFFFFu, v);
 #pragma unroll
@@ -328,65 +362,67 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __res
                 uint32_t base = 0;
                 if (v && static_cast<int>(lane) == leader) {
                     base = sm.warp_cnt[warp][d];
-                    sm.warp_cnt[warp][d] = base + __popc(peers);
+                    sm.warp_cnt[warp][d] = static_cast<uint16_t>(base + __popc(peers));
                 }
                 base = __shfl_sync(0xFFFFFFFFu, base, leader);
                 rank[j] = base + __popc(peers & lt_mask);
-                dig[j] = v ? d : static_cast<uint32_t>(kRadix);
                 __syncwarp();
             }
         }
-        __syncthreads();  // tile read and ranked: its buffer may be refilled
-        if (tid == 0) issue(t + 2);
+        __syncthreads();  // tile read and ranked: its buffer may take the staged tile
         // thread d: the tile total of digit d (the previous tile's total moves
-        // into the running offset), per-warp prefixes when ranked stably, and
-        // the scan within its group of 32 digits
+        // into the running offset), per-warp prefixes when ranked stably, the
+        // digit's first staged position and its output base
         {
             uint32_t s = 0;
             if (!stable) {
-                s = sm.warp_cnt[0][tid];
-                sm.warp_cnt[0][tid] = 0;
+                s = sm.cnt[tid];
+                sm.cnt[tid] = 0;
             } else {
 #pragma unroll
                 for (int w = 0; w < kRsWarps; ++w) {
                     const uint32_t c = sm.warp_cnt[w][tid];
-                    sm.warp_cnt[w][tid] = s;
+                    sm.warp_cnt[w][tid] = static_cast<uint16_t>(s);
                     s += c;
                 }
             }
-            sm.running[tid] += sm.tot[tid];
+            const uint32_t run = sm.running[tid] + sm.tot[tid];
+            sm.running[tid] = run;
             sm.tot[tid] = s;
             const uint32_t incl = warp_inclusive_scan(s);
-            sm.tile_off[tid] = incl - s;
-            if (lane == 31) sm.grp_off[warp] = incl;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t x = lane < kRadix / 32 ? sm.grp_off[lane] : 0u;
-            const uint32_t xi = warp_inclusive_scan(x);
-            if (lane < kRadix / 32) sm.grp_off[lane] = xi - x;
+            if (lane == 31) sm.grp_tot[warp] = incl;
+            __syncthreads();
+            // every warp scans the group totals itself, so thread d can place its
+            // digit without another barrier: one lookup per item below, not three
+            const uint32_t x = lane < kRadix / 32 ? sm.grp_tot[lane] : 0u;
+            const uint32_t grp = __shfl_sync(0xFFFFFFFFu, warp_inclusive_scan(x) - x, warp);
+            const uint32_t first_pos = grp + incl - s;
+            sm.tile_off[tid] = first_pos;
+            sm.out_base[tid] = run - first_pos;
         }
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < kRsIPT; ++j) {
-            const uint32_t d = dig[j];
-            if (d < kRadix) {
-                uint32_t pos = sm.grp_off[d >> 5] + sm.tile_off[d] + rank[j];
+            if (full || warp * 32 * kRsIPT + j * 32 + lane < count) {
+                const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
+                uint32_t pos = sm.tile_off[d] + rank[j];
                 if (stable) pos += sm.warp_cnt[warp][d];
-                sm.stage[pos] = e[j];
-                if constexpr (PAY) sm.stage_pay[pos] = p[j];
+                sm.in[b][pos] = e[j];
+                if constexpr (PAY) sm.in_pay[b][pos] = p[j];
             }
         }
         __syncthreads();
         for (uint32_t q = tid; q < count; q += blockDim.x) {
-            const uint64_t x = sm.stage[q];
+            const uint64_t x = sm.in[b][q];
             const uint32_t d = static_cast<uint32_t>((x >> shift) & (kRadix - 1));
-            const uint32_t g = sm.running[d] + (q - sm.grp_off[d >> 5] - sm.tile_off[d]);
+            const uint32_t g = sm.out_base[d] + q;
             dst[g] = x;
-            if constexpr (PAY) dst_pay[g] = sm.stage_pay[q];
+            if constexpr (PAY) dst_pay[g] = sm.in_pay[b][q];
         }
         if (stable)
             for (int i = tid; i < kRsWarps * kRadix; i += blockDim.x) (&sm.warp_cnt[0][0])[i] = 0;
+        __syncthreads();  // the tile is written out and the counters are reset: refill its buffer
+        if (tid == 0) issue(t + 2);
     }
     if (__any_sync(0xFFFFFFFFu, failed) && lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
 }
@@ -935,11 +971,13 @@ __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
 // bucket.  A tag takes the first empty slot circularly from slot
 // align_down(fp & (bs-1), tagsPerWord) -- exactly the order in which the
 // reference's tryInsertAtBucket scans words and lanes (CuckooFilter.cuh:859-904)
-// -- claimed with one compare-and-swap on the mask, then written into the slot
+// -- claimed with one atomic AND on the mask, then written into the slot
 // with a plain store (the claim makes the slot the thread's own).  Tags whose
 // bucket is full go to `next`: keyed by the alternate bucket in round 1,
 // unchanged (for eviction) in round 2.
-template <class C>
+// PAY: entries carry payloads (key positions; `pay`, `next_pay` and `bitmap`
+// are used only then).
+template <class C, bool PAY>
 __global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                             const uint32_t* start, uint64_t nseg, int sb_log2,
                                                             int round, uint64_t* next, uint32_t* next_pay,
@@ -984,15 +1022,15 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const
         constexpr int U = 8;
         for (uint32_t base = lo; base < hi; base += blockDim.x * U) {
             uint64_t ev[U];
-            uint32_t pv[U];
+            uint32_t pv[PAY ? U : 1];
 #pragma unroll
             for (int j = 0; j < U; ++j) {
                 const uint32_t k = base + j * blockDim.x + tid;
                 ev[j] = 0;
-                pv[j] = 0;
+                if constexpr (PAY) pv[j] = 0;
                 if (k < hi) {
                     ev[j] = ent[k];
-                    if (pay) pv[j] = pay[k];
+                    if constexpr (PAY) pv[j] = pay[k];
                 }
             }
             uint32_t fwd_mask = 0;
@@ -1014,8 +1052,10 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const
                     else
                         off = __ffs(static_cast<int>(rot)) - 1;
                     const uint32_t slot = (s0 + off) & (C::bs - 1);
-                    const M old = atomicCAS(&mask[lb], m, m & ~(static_cast<M>(1) << slot));
-                    if (old == m) {
+                    // claim the slot alone: only a claim of the same slot can fail
+                    const M bit = static_cast<M>(1) << slot;
+                    const M old = atomicAnd(&mask[lb], ~bit);
+                    if (old & bit) {
                         uint8_t* dst = seg_bytes + (static_cast<uint64_t>(lb) * C::bucket_bytes + slot * TB);
                         if constexpr (TB == 1)
                             *dst = static_cast<uint8_t>(fp);
@@ -1030,7 +1070,7 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const
                 }
                 if (ok) {
                     ++n_ok;
-                    if (bitmap) atomicOr(&bitmap[pv[j] >> 5], 1u << (pv[j] & 31));
+                    if constexpr (PAY) atomicOr(&bitmap[pv[j] >> 5], 1u << (pv[j] & 31));
                 } else {
                     fwd_mask |= 1u << j;
                 }
@@ -1056,7 +1096,7 @@ __global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const
                         uint64_t b = ev[j] >> C::bits;
                         if (round == 1) b = alt_bucket<C>(b, fp, t.nb_mask);
                         next[o] = pack_entry<C>(b, fp);
-                        if (pay) next_pay[o] = pv[j];
+                        if constexpr (PAY) next_pay[o] = pv[j];
                         ++o;
                     }
                 }
