@@ -308,7 +308,8 @@ struct Launchers {
         // one CTA per segment (measured faster on B200 than one wave of CTAs
         // striding over the segments)
         const int grid = static_cast<int>(g.nseg < 0x7FFFFFFFull ? g.nseg : 0x7FFFFFFFull);
-        { (payload ? kern_pay : kern)<<<grid, kSegThreads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr,
+        const int threads = OP == SEG_INSERT ? kSegInsertThreads : kSegThreads;
+        { (payload ? kern_pay : kern)<<<grid, threads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr,
                                                                      w.start, g.nseg, g.sb_log2, round, w.ent[other],
                                                                      payload ? w.pay[other] : nullptr, &w.cnt[round - 1],
                                                                      payload ? w.bitmap : nullptr); CF_COUNT_LAUNCH(); }

@@ -35,8 +35,22 @@ constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kRsIPT = 16;
-constexpr int kRsTile = kRsThreads * kRsIPT;
+// Entries per thread of a scatter tile: 24 without payloads (a 6144-entry
+// tile, two CTAs per SM in 107 KB of shared memory), 16 with payloads (the
+// 4-byte payload buffers need the room).  On B200 a 2^31-entry pass took
+// 7.97 ms with 24 against 8.58 ms with 16.
+template <int PAY>
+constexpr int rs_ipt() {
+    return PAY ? 16 : 24;
+}
+template <int PAY>
+constexpr int rs_tile() {
+    return kRsThreads * rs_ipt<PAY>();
+}
+// Every CTA chunk of a radix pass is a multiple of this many entries, which
+// both tile sizes divide.
+constexpr int kRsChunkAlign = 12288;
+static_assert(kRsChunkAlign % rs_tile<0>() == 0 && kRsChunkAlign % rs_tile<1>() == 0, "chunk alignment");
 constexpr int kRsHistThreads = 512;
 // Histogram CTAs per scatter CTA: each counts one part of the scatter CTA's
 // chunk, so the histogram pass runs on three times the scatter's grid.
@@ -44,6 +58,7 @@ constexpr int kRsHistSub = 3;
 static_assert(kRsThreads == kRadix, "the scatter's per-digit phases give one thread per digit");
 constexpr int kSegBytes = 65536;
 constexpr int kSegThreads = 256;
+constexpr int kSegInsertThreads = 256;
 
 template <class C>
 __device__ __forceinline__ uint64_t pack_entry(uint64_t bucket, uint32_t fp) {
@@ -70,7 +85,7 @@ __device__ __forceinline__ uint64_t item_count(uint64_t n, const unsigned long l
 
 __device__ __forceinline__ uint64_t chunk_of(uint64_t n, uint32_t parts) {
     const uint64_t per = (n + parts - 1) / parts;
-    return (per + kRsTile - 1) / kRsTile * kRsTile;
+    return (per + kRsChunkAlign - 1) / kRsChunkAlign * kRsChunkAlign;
 }
 
 // Digit histogram of each scatter CTA's contiguous chunk, counted by
@@ -226,8 +241,9 @@ static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t 
 // staged and written out.
 template <int PAY>
 struct RsScatterSmem {
-    uint64_t in[2][kRsTile];                      // bulk-copy double buffer (entries), then the staged tile
-    uint32_t in_pay[2][PAY ? kRsTile : 1];        // payloads: bulk-copied (PAY 2), then staged
+    static constexpr int TILE = rs_tile<PAY>();
+    uint64_t in[2][TILE];                      // bulk-copy double buffer (entries), then the staged tile
+    uint32_t in_pay[2][PAY ? TILE : 1];        // payloads: bulk-copied (PAY 2), then staged
     uint32_t cnt[kRadix];                         // digit counts of the tile (ranking by atomics)
     uint16_t warp_cnt[kRsWarps][kRadix];          // stable ranking: per-warp digit counts, then their warp prefix
     uint32_t running[kRadix];                     // next output position per digit
@@ -239,10 +255,10 @@ struct RsScatterSmem {
 };
 
 // One LSD pass over packed entries: scatter them to dst by digit, using the
-// scanned histogram as the CTA's starting offset per digit.  Full 4096-entry tiles
+// scanned histogram as the CTA's starting offset per digit.  Full tiles
 // arrive by bulk copy into a double buffer (the copy of tile t+2 is issued
 // when tile t has been written out, so tile t+1 is in flight while tile t is
-// worked on).  Each tile is ranked in shared memory (16 entries per thread),
+// worked on).  Each tile is ranked in shared memory (rs_ipt entries per thread),
 // staged in digit order in its own buffer and written out as contiguous runs.
 //
 // The sort only has to group entries by segment, so a pass needs to keep the
@@ -256,11 +272,13 @@ struct RsScatterSmem {
 // PAY: 0 = no payload, 1 = the payload of entry i is i itself, 2 = payloads
 // read from src_pay.
 template <int PAY>
-__global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __restrict__ src,
+__global__ void __launch_bounds__(kRsThreads, 2) k_rs_scatter(const uint64_t* __restrict__ src,
                                                               const uint32_t* __restrict__ src_pay, uint64_t n,
                                                               const unsigned long long* n_dev, int shift, int lo_bits,
                                                               const uint32_t* offs, uint64_t* __restrict__ dst,
                                                               uint32_t* __restrict__ dst_pay, unsigned long long* err) {
+    constexpr int IPT = rs_ipt<PAY>();
+    constexpr int TILE = rs_tile<PAY>();
     extern __shared__ __align__(128) unsigned char rs_raw[];
     RsScatterSmem<PAY>& sm = *reinterpret_cast<RsScatterSmem<PAY>*>(rs_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -269,8 +287,8 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __
     const uint64_t chunk = chunk_of(m, gridDim.x);
     const uint64_t lo = blockIdx.x * chunk;
     const uint64_t hi = lo + chunk < m ? lo + chunk : m;
-    const uint32_t ntile = lo < hi ? static_cast<uint32_t>((hi - lo + kRsTile - 1) / kRsTile) : 0u;
-    const uint32_t nfull = lo < hi ? static_cast<uint32_t>((hi - lo) / kRsTile) : 0u;  // only the last can be partial
+    const uint32_t ntile = lo < hi ? static_cast<uint32_t>((hi - lo + TILE - 1) / TILE) : 0u;
+    const uint32_t nfull = lo < hi ? static_cast<uint32_t>((hi - lo) / TILE) : 0u;  // only the last can be partial
     const int lo_shift = shift - lo_bits;
     const uint64_t lo_mask = (1ull << lo_bits) - 1ull;
     for (int d = tid; d < kRadix; d += blockDim.x) {
@@ -289,11 +307,11 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __
     auto issue = [&](uint32_t t) {
         if (t >= nfull) return;
         const uint32_t b = t & 1u;
-        const uint64_t i0 = lo + static_cast<uint64_t>(t) * kRsTile;
+        const uint64_t i0 = lo + static_cast<uint64_t>(t) * TILE;
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&sm.bar[b], kRsTile * 8u + (PAY == 2 ? kRsTile * 4u : 0u));
-        bulk_g2s(sm.in[b], src + i0, kRsTile * 8u, &sm.bar[b]);
-        if constexpr (PAY == 2) bulk_g2s(sm.in_pay[b], src_pay + i0, kRsTile * 4u, &sm.bar[b]);
+        mbar_arrive_expect_tx(&sm.bar[b], TILE * 8u + (PAY == 2 ? TILE * 4u : 0u));
+        bulk_g2s(sm.in[b], src + i0, TILE * 8u, &sm.bar[b]);
+        if constexpr (PAY == 2) bulk_g2s(sm.in_pay[b], src_pay + i0, TILE * 4u, &sm.bar[b]);
     };
     if (tid == 0) {
         issue(0);
@@ -302,28 +320,28 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __
     bool failed = false;
     for (uint32_t t = 0; t < ntile; ++t) {
         const uint32_t b = t & 1u;
-        const uint64_t tb = lo + static_cast<uint64_t>(t) * kRsTile;
+        const uint64_t tb = lo + static_cast<uint64_t>(t) * TILE;
         const bool full = t < nfull;
-        const uint32_t count = full ? static_cast<uint32_t>(kRsTile) : static_cast<uint32_t>(hi - tb);
-        uint64_t e[kRsIPT];
-        uint32_t p[kRsIPT], rank[kRsIPT];
+        const uint32_t count = full ? static_cast<uint32_t>(TILE) : static_cast<uint32_t>(hi - tb);
+        uint64_t e[IPT];
+        uint32_t p[IPT], rank[IPT];
         uint64_t first, last;
         if (full) {
             if (!mbar_wait(&sm.bar[b], (t >> 1) & 1u, kMbarPollLimit)) failed = true;
 #pragma unroll
-            for (int j = 0; j < kRsIPT; ++j) {
-                const uint32_t idx = warp * 32 * kRsIPT + j * 32 + lane;
+            for (int j = 0; j < IPT; ++j) {
+                const uint32_t idx = warp * 32 * IPT + j * 32 + lane;
                 e[j] = sm.in[b][idx];
                 p[j] = 0;
                 if constexpr (PAY == 1) p[j] = static_cast<uint32_t>(tb + idx);
                 if constexpr (PAY == 2) p[j] = sm.in_pay[b][idx];
             }
             first = sm.in[b][0];
-            last = sm.in[b][kRsTile - 1];
+            last = sm.in[b][TILE - 1];
         } else {
 #pragma unroll
-            for (int j = 0; j < kRsIPT; ++j) {
-                const uint64_t i = tb + warp * 32 * kRsIPT + j * 32 + lane;
+            for (int j = 0; j < IPT; ++j) {
+                const uint64_t i = tb + warp * 32 * IPT + j * 32 + lane;
                 e[j] = 0;
                 p[j] = 0;
                 if (i < hi) {
@@ -340,16 +358,16 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __
         if (!stable) {
             // rank = arrival order within the digit, counted in cnt
 #pragma unroll
-            for (int j = 0; j < kRsIPT; ++j) {
-                const bool v = full || warp * 32 * kRsIPT + j * 32 + lane < count;
+            for (int j = 0; j < IPT; ++j) {
+                const bool v = full || warp * 32 * IPT + j * 32 + lane < count;
                 const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
                 rank[j] = v ? atomicAdd(&sm.cnt[d], 1u) : 0u;
             }
         } else {
             // rank = lane order within the warp's row, rows in order, warps in order
 #pragma unroll
-            for (int j = 0; j < kRsIPT; ++j) {
-                const bool v = full || warp * 32 * kRsIPT + j * 32 + lane < count;
+            for (int j = 0; j < IPT; ++j) {
+                const bool v = full || warp * 32 * IPT + j * 32 + lane < count;
                 const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
                 uint32_t peers = __ballot_sync(0xFFFFFFFFu, v);
 #pragma unroll
@@ -402,8 +420,8 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_rs_scatter(const uint64_t* __
         }
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < kRsIPT; ++j) {
-            if (full || warp * 32 * kRsIPT + j * 32 + lane < count) {
+        for (int j = 0; j < IPT; ++j) {
+            if (full || warp * 32 * IPT + j * 32 + lane < count) {
                 const uint32_t d = static_cast<uint32_t>((e[j] >> shift) & (kRadix - 1));
                 uint32_t pos = sm.tile_off[d] + rank[j];
                 if (stable) pos += sm.warp_cnt[warp][d];
@@ -960,9 +978,18 @@ __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
 #pragma unroll
     for (int j = 0; j < C::nchunks; ++j) {
         const uint64_t z = zero_lanes<C::bits>(bw[j]);
+        if constexpr (C::bits == 16) {
+            // the four lane flags (bits 15, 31, 47, 63) gathered into bits 48..51
+            // by one multiply: flag l lands at 48 + l, every other product term
+            // below bit 48 or above bit 63
+            const uint64_t f = (z >> 15) & 0x0001000100010001ULL;
+            const uint64_t g = (f * ((1ULL << 48) | (1ULL << 33) | (1ULL << 18) | (1ULL << 3))) >> 48;
+            m |= static_cast<SlotMask<C>>(g & 0xFu) << (j * 4);
+        } else {
 #pragma unroll
-        for (int l = 0; l < C::lanes_per_chunk; ++l)
-            m |= static_cast<SlotMask<C>>((z >> (l * C::bits + C::bits - 1)) & 1u) << (j * C::lanes_per_chunk + l);
+            for (int l = 0; l < C::lanes_per_chunk; ++l)
+                m |= static_cast<SlotMask<C>>((z >> (l * C::bits + C::bits - 1)) & 1u) << (j * C::lanes_per_chunk + l);
+        }
     }
     return m;
 }
@@ -978,7 +1005,7 @@ __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
 // PAY: entries carry payloads (key positions; `pay`, `next_pay` and `bitmap`
 // are used only then).
 template <class C, bool PAY>
-__global__ void __launch_bounds__(kSegThreads, 3) k_seg_insert(DevTable t, const uint64_t* ent, const uint32_t* pay,
+__global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                             const uint32_t* start, uint64_t nseg, int sb_log2,
                                                             int round, uint64_t* next, uint32_t* next_pay,
                                                             unsigned long long* next_count, uint32_t* bitmap) {
