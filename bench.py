@@ -869,17 +869,32 @@ def run_kmer(args) -> dict:
     dev = torch.device("cuda", 0)
     n_bases = 1 << args.kmer_bases_log2
     t0 = time.perf_counter()
-    dna = markov_dna(n_bases, 1 << 14, args.batched_seed, dev)
-    kmers = torch.unique(canonical_kmers(dna))
     g = torch.Generator(device=dev)
     g.manual_seed(args.batched_seed + 1)
-    kmers = kmers[torch.randperm(kmers.numel(), generator=g, device=dev)]
-    queries = canonical_kmers(mutate(dna, 0.01, args.batched_seed + 2))
+    if args.kmer_file:
+        # a real k-mer set in the reference's binary format: inserted in a seeded
+        # shuffle; queries are every k-mer of the set (positives) plus as many
+        # splitmix64 keys (negatives up to the false-positive rate)
+        from cuckoo_b200.kmer import read_kmer_file
+
+        host = read_kmer_file(args.kmer_file)
+        kmers = torch.unique(torch.from_numpy(host.view(np.int64)).to(dev))
+        kmers = kmers[torch.randperm(kmers.numel(), generator=g, device=dev)]
+        neg = splitmix64_segments(np.array([args.batched_seed + 3], np.int64), np.array([kmers.numel()], np.int64),
+                                  np.array([0], np.int64), dev)
+        queries = torch.cat([kmers, neg])
+        data = f"k-mer file {os.path.basename(args.kmer_file)} ({host.size} k-mers); queries: the set plus as many splitmix64 keys"
+        n_bases = 0
+    else:
+        dna = markov_dna(n_bases, 1 << 14, args.batched_seed, dev)
+        kmers = torch.unique(canonical_kmers(dna))
+        kmers = kmers[torch.randperm(kmers.numel(), generator=g, device=dev)]
+        queries = canonical_kmers(mutate(dna, 0.01, args.batched_seed + 2))
+        data = (f"synthetic: 2^{args.kmer_bases_log2}-base order-3 Markov DNA (Dirichlet(1) rows), canonical "
+                "31-mers 2-bit MSB-first, deduplicated; queries from a 1%-substituted copy")
     gen_s = time.perf_counter() - t0
     out = {"form": "kmer", "metric": "insert Gkeys/s per load step; lookup Gkeys/s and hit rate",
-           "unit": "Gkeys/s", "n_gpus": 1, "dtype": "u64",
-           "data": f"synthetic: 2^{args.kmer_bases_log2}-base order-3 Markov DNA (Dirichlet(1) rows), canonical "
-                   "31-mers 2-bit MSB-first, deduplicated; queries from a 1%-substituted copy",
+           "unit": "Gkeys/s", "n_gpus": 1, "dtype": "u64", "data": data,
            "config": {"workload": "kmer", "bases": n_bases, "distinct_kmers": int(kmers.numel()),
                       "query_windows": int(queries.numel()), "generation_s": gen_s}, "filters": []}
     stream = torch.cuda.current_stream()
@@ -1091,6 +1106,9 @@ def main() -> None:
     ap.add_argument("--cpu-scale", type=int, default=27, help="log2 slots of the CPU-baseline sample")
     ap.add_argument("--ref-scale", type=int, default=25, help="log2 slots of each reference-arm CPU step")
     ap.add_argument("--kmer-bases-log2", type=int, default=28)
+    ap.add_argument("--kmer-file", default=None,
+                    help="--form kmer: insert the k-mers of this file (u64 count + u64 2-bit k-mers, the "
+                         "reference's k-mer benchmark format) instead of synthetic DNA")
     ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid"), default="plain",
                     help="batched: the filter-set form over 4096 uneven filters; served: the multi-tenant "
                          "continuous-batching form (each its own JSON line)")
