@@ -105,15 +105,19 @@ struct Cfg {
     static constexpr int word_bytes = WB;
     static constexpr int bucket_bytes = BS * BITS / 8;
     static constexpr int nchunks = bucket_bytes / 8;     // 64-bit chunks per bucket
-    static constexpr int lanes_per_chunk = 64 / BITS;    // tags per 64-bit chunk
-    static constexpr int tpw = WB * 8 / BITS;            // tags per CAS word
-    static constexpr int wc = BS / tpw;                  // CAS words per bucket
+    static constexpr int lanes_per_chunk = 64 / BITS;    // tags per 64-bit chunk (the unit of every atomic here)
+    static constexpr int tpw = WB * 8 / BITS;            // tags per WordType word (the reference's scan unit)
+    static constexpr int wc = BS / tpw;                  // WordType words per bucket
+    // Slot scans start at align_down(tag & (bs-1), tpw).  With 64-bit words a
+    // scan can go chunk by chunk; with 32-bit words it goes slot by slot.
+    static constexpr bool chunk_scan = tpw == lanes_per_chunk;
     static constexpr uint32_t tag_mask = BITS == 32 ? 0xFFFFFFFFu : ((1u << BITS) - 1u);
     static_assert(KB == 4 || KB == 8, "key must be 4 or 8 bytes");
     static_assert(BITS == 8 || BITS == 16 || BITS == 32, "tag must be 8, 16 or 32 bits");
     static_assert((BS & (BS - 1)) == 0, "bucket size must be a power of two");
     static_assert(bucket_bytes >= 8 && bucket_bytes % 8 == 0, "bucket must be a whole number of 8-byte chunks");
-    static_assert(WB == 8, "64-bit CAS words");
+    static_assert(WB == 4 || WB == 8, "WordType is uint32_t or uint64_t");
+    static_assert(BITS <= WB * 8, "a tag must fit in one word");
     static_assert(BS % tpw == 0, "bucket size must be a multiple of tags per word");
     static_assert(BS <= 64, "at most 64 slots per bucket");
     using Key = typename std::conditional<KB == 8, uint64_t, uint32_t>::type;

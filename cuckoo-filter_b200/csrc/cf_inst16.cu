@@ -1,4 +1,5 @@
-// cf_inst16.cu -- kernel instantiations for 16-bit tags (64-bit CAS words).
+// cf_inst16.cu -- kernel instantiations for 16-bit tags (WordType uint64_t, and uint32_t for the reference's
+// word-width comparison geometry).
 #include "cf_registry.cuh"
 
 namespace cfb {
@@ -12,6 +13,8 @@ void register_bits16(std::vector<OpsTable>& v) {
     v.push_back(Launchers<Cfg<4, 16, 16, 8>>::table());
     v.push_back(Launchers<Cfg<8, 16, 32, 8>>::table());
     v.push_back(Launchers<Cfg<4, 16, 32, 8>>::table());
+    v.push_back(Launchers<Cfg<8, 16, 16, 4>>::table());  // WordType uint32_t
+    v.push_back(Launchers<Cfg<4, 16, 16, 4>>::table());  // WordType uint32_t
 }
 
 }  // namespace cfb

@@ -102,10 +102,66 @@ __device__ __forceinline__ int first_word(uint32_t words, int sw) {
     }
 }
 
+// Per-bucket slot mask type: one bit per slot.
+template <class C>
+using SlotMask = typename std::conditional<(C::bs > 32), unsigned long long, unsigned int>::type;
+
+// Bit s set when slot s of bucket image c holds `tag` (0: the empty slots).
+template <class C>
+__device__ __forceinline__ SlotMask<C> slots_holding(const uint64_t (&c)[C::nchunks], uint32_t tag) {
+    const uint64_t rep = replicate<C::bits>(tag);
+    SlotMask<C> m = 0;
+#pragma unroll
+    for (int j = 0; j < C::nchunks; ++j) {
+        const uint64_t z = zero_lanes<C::bits>(c[j] ^ rep);
+#pragma unroll
+        for (int l = 0; l < C::lanes_per_chunk; ++l)
+            m |= static_cast<SlotMask<C>>((z >> (l * C::bits + C::bits - 1)) & 1u) << (j * C::lanes_per_chunk + l);
+    }
+    return m;
+}
+
+// First slot set in m, circularly from slot s0 (m != 0).
+template <class C>
+__device__ __forceinline__ uint32_t first_slot_from(SlotMask<C> m, uint32_t s0) {
+    constexpr int kBits = 8 * sizeof(SlotMask<C>);
+    constexpr SlotMask<C> full = C::bs == kBits ? ~static_cast<SlotMask<C>>(0)
+                                                : ((static_cast<SlotMask<C>>(1) << (C::bs % kBits)) - 1);
+    const SlotMask<C> rot = s0 ? (((m >> s0) | (m << (C::bs - s0))) & full) : m;
+    uint32_t off;
+    if constexpr (sizeof(SlotMask<C>) == 8)
+        off = __ffsll(static_cast<long long>(rot)) - 1;
+    else
+        off = __ffs(static_cast<int>(rot)) - 1;
+    return (s0 + off) & (C::bs - 1);
+}
+
+// First slot of the reference's word-by-word scan (start word
+// (tag & (bs-1)) / tpw, lowest lane first) among the slots set in m.
+template <class C>
+__device__ __forceinline__ uint32_t scan_slot(SlotMask<C> m, uint32_t tag) {
+    return first_slot_from<C>(m, ((tag & (C::bs - 1)) / C::tpw) * C::tpw);
+}
+
 // tryInsertAtBucket on a bucket whose current image is in c (refreshed on
 // compare-and-swap failure).  Returns true when fp was stored.
 template <class C>
 __device__ bool try_insert(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp, bool& err) {
+    if constexpr (!C::chunk_scan) {
+        for (int it = 0; it < kCasRetryLimit; ++it) {
+            const SlotMask<C> m = slots_holding<C>(c, 0);
+            if (!m) return false;
+            const uint32_t slot = scan_slot<C>(m, fp);
+            const int w = static_cast<int>(slot / C::lanes_per_chunk);
+            const uint64_t cur = pick(c, w);
+            const uint64_t desired = cur | (static_cast<uint64_t>(fp) << ((slot % C::lanes_per_chunk) * C::bits));
+            const uint64_t old = cas64(bw + w, cur, desired);
+            if (old == cur) return true;
+            put(c, w, old);
+        }
+        err = true;
+        return false;
+    }
     const int sw = static_cast<int>((fp & (C::bs - 1)) / C::tpw);
     for (int it = 0; it < kCasRetryLimit; ++it) {
         uint32_t words = 0;
@@ -130,6 +186,15 @@ __device__ bool try_insert(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp,
 template <class C>
 __device__ __forceinline__ bool plan_insert(const uint64_t (&c)[C::nchunks], uint32_t fp, int& w, uint64_t& cur,
                                             uint64_t& desired) {
+    if constexpr (!C::chunk_scan) {
+        const SlotMask<C> m = slots_holding<C>(c, 0);
+        if (!m) return false;
+        const uint32_t slot = scan_slot<C>(m, fp);
+        w = static_cast<int>(slot / C::lanes_per_chunk);
+        cur = pick(c, w);
+        desired = cur | (static_cast<uint64_t>(fp) << ((slot % C::lanes_per_chunk) * C::bits));
+        return true;
+    }
     const int sw = static_cast<int>((fp & (C::bs - 1)) / C::tpw);
     uint32_t words = 0;
 #pragma unroll
@@ -145,9 +210,24 @@ __device__ __forceinline__ bool plan_insert(const uint64_t (&c)[C::nchunks], uin
 // tryRemoveAtBucket: clear the first slot holding fp.
 template <class C>
 __device__ bool try_remove(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp, bool& err) {
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    if constexpr (!C::chunk_scan) {
+        for (int it = 0; it < kCasRetryLimit; ++it) {
+            const SlotMask<C> m = slots_holding<C>(c, fp);
+            if (!m) return false;
+            const uint32_t slot = scan_slot<C>(m, fp);
+            const int w = static_cast<int>(slot / C::lanes_per_chunk);
+            const uint64_t cur = pick(c, w);
+            const uint64_t desired = cur & ~(lane_mask << ((slot % C::lanes_per_chunk) * C::bits));
+            const uint64_t old = cas64(bw + w, cur, desired);
+            if (old == cur) return true;
+            put(c, w, old);
+        }
+        err = true;
+        return false;
+    }
     const int sw = static_cast<int>((fp & (C::bs - 1)) / C::tpw);
     const uint64_t rep = replicate<C::bits>(fp);
-    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
     for (int it = 0; it < kCasRetryLimit; ++it) {
         uint32_t words = 0;
 #pragma unroll
@@ -178,8 +258,8 @@ __device__ __forceinline__ bool has_tag(const uint64_t (&c)[C::nchunks], uint32_
 template <class C>
 __device__ uint32_t exchange_slot(uint64_t* bw, uint32_t slot, uint32_t v, bool& err) {
     constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
-    const int w = static_cast<int>(slot / C::tpw);
-    const int sh = static_cast<int>(slot % C::tpw) * C::bits;
+    const int w = static_cast<int>(slot / C::lanes_per_chunk);
+    const int sh = static_cast<int>(slot % C::lanes_per_chunk) * C::bits;
     uint64_t cur = load_word_rlx(bw + w);
     for (int it = 0; it < kCasRetryLimit; ++it) {
         const uint64_t desired = (cur & ~(lane_mask << sh)) | (static_cast<uint64_t>(v) << sh);
@@ -281,8 +361,8 @@ __device__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, uint64_t othe
     load_rlx<C::bucket_bytes>(sbw, snap);
     for (uint32_t i = 0; i < ncand; ++i) {
         const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * i) & (C::bs - 1));
-        const int w = static_cast<int>(slot / C::tpw);
-        const int sh = static_cast<int>(slot % C::tpw) * C::bits;
+        const int w = static_cast<int>(slot / C::lanes_per_chunk);
+        const int sh = static_cast<int>(slot % C::lanes_per_chunk) * C::bits;
         uint64_t word = pick(snap, w);
         const uint32_t cand = static_cast<uint32_t>((word >> sh) & lane_mask);
         uint64_t c[C::nchunks];

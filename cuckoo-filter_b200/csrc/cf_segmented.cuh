@@ -651,8 +651,8 @@ __global__ void __launch_bounds__(256) k_evict_bfs_coop(DevTable t, const uint64
         }
         uint64_t* sbw = bucket_words<C>(t, start);
         const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * gl) & (C::bs - 1));
-        const int sw = static_cast<int>(slot / C::tpw);
-        const int sh = static_cast<int>(slot % C::tpw) * C::bits;
+        const int sw = static_cast<int>(slot / C::lanes_per_chunk);
+        const int sh = static_cast<int>(slot % C::lanes_per_chunk) * C::bits;
         uint32_t cand = 0;
         uint64_t ab = 0;
         bool room = false;
@@ -770,8 +770,8 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
     auto select = [&]() -> int {
         for (; i < NC; ++i) {
             const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * i) & (C::bs - 1));
-            sw = static_cast<int>(slot / C::tpw);
-            sh = (slot % C::tpw) * C::bits;
+            sw = static_cast<int>(slot / C::lanes_per_chunk);
+            sh = (slot % C::lanes_per_chunk) * C::bits;
             cand = static_cast<uint32_t>((pick(snap, sw) >> sh) & lane_mask);
             if (cand == 0) {  // reference :980-985: the slot is free, insert fp into the start bucket
                 if (plan_insert<C>(snap, fp, w, exp, des)) {
@@ -960,10 +960,6 @@ __global__ void __launch_bounds__(256) k_evict_list(DevTable t, const uint64_t* 
     flush_counter(&t.ctr[CTR_LOST], st.lost);
     if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
 }
-
-// Per-bucket empty-slot mask type: one bit per slot.
-template <class C>
-using SlotMask = typename std::conditional<(C::bs > 32), unsigned long long, unsigned int>::type;
 
 // Shared memory of k_seg_insert: the staged segment plus one slot mask per bucket.
 template <class C>

@@ -54,7 +54,7 @@ typedef struct cf_config {
     uint32_t key_bytes;       /* sizeof(T): 4 (uint32_t) or 8 (uint64_t) */
     uint32_t bits_per_tag;    /* bitsPerTag: 8, 16 or 32 */
     uint32_t bucket_size;     /* bucketSize: slots per bucket, power of two, 8..64 bytes per bucket */
-    uint32_t word_bytes;      /* sizeof(WordType): 8 */
+    uint32_t word_bytes;      /* sizeof(WordType): 8, or 4 for the (8, 16), (16, 16) and (32, 8) tag/bucket geometries */
     uint32_t eviction_policy; /* cf_eviction */
     uint32_t max_evictions;   /* maxEvictions: 1..512 */
     uint32_t block_size;      /* blockSize: threads per block, multiple of 32, <= 512; 0 = tuned */

@@ -270,6 +270,11 @@ REF_GPU_CONFIGS = {
     (8, 16, 16, POLICY_BFS, 16): 8,
     (8, 32, 8, POLICY_DFS, 16): 9,
     (8, 32, 8, POLICY_BFS, 16): 10,
+    # 32-bit WordType: (key_bytes, bits, bucket_size, policy, max_evictions, word_bytes)
+    (8, 8, 16, POLICY_DFS, 500, 4): 11,
+    (8, 8, 16, POLICY_BFS, 500, 4): 12,
+    (8, 16, 16, POLICY_DFS, 500, 4): 13,
+    (8, 16, 16, POLICY_BFS, 16, 4): 14,
 }
 
 _ref_gpu = None
@@ -305,8 +310,9 @@ def ref_gpu():
 class RefGpuFilter:
     """The reference's CuckooFilter<Config> (managed-memory object) on cuda:0."""
 
-    def __init__(self, key_bytes, bits, bucket_size, policy, max_evictions, capacity):
-        self.cfg = REF_GPU_CONFIGS[(key_bytes, bits, bucket_size, policy, max_evictions)]
+    def __init__(self, key_bytes, bits, bucket_size, policy, max_evictions, capacity, word_bytes=8):
+        key = (key_bytes, bits, bucket_size, policy, max_evictions)
+        self.cfg = REF_GPU_CONFIGS[key if word_bytes == 8 else key + (word_bytes,)]
         self.L = ref_gpu()
         self.h = self.L.refg_create(self.cfg, capacity)
         if not self.h:

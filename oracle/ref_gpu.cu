@@ -30,6 +30,12 @@ using XorU64_16_DFS_E16 = CuckooConfig<uint64_t, 16, 16, 256, 16, XorAltBucketPo
 using XorU64_16_BFS_E16 = CuckooConfig<uint64_t, 16, 16, 256, 16, XorAltBucketPolicy, EvictionPolicy::BFS>;
 using XorU64_32_DFS_E16 = CuckooConfig<uint64_t, 32, 16, 256, 8, XorAltBucketPolicy, EvictionPolicy::DFS>;
 using XorU64_32_BFS_E16 = CuckooConfig<uint64_t, 32, 16, 256, 8, XorAltBucketPolicy, EvictionPolicy::BFS>;
+// 32-bit WordType (the reference's word-width comparison, benchmark/cuckoo_atomics_comparison.cu)
+using XorU64_8_DFS_W32 = CuckooConfig<uint64_t, 8, 500, 256, 16, XorAltBucketPolicy, EvictionPolicy::DFS, uint32_t>;
+using XorU64_8_BFS_W32 = CuckooConfig<uint64_t, 8, 500, 256, 16, XorAltBucketPolicy, EvictionPolicy::BFS, uint32_t>;
+using XorU64_16_DFS_W32 = CuckooConfig<uint64_t, 16, 500, 256, 16, XorAltBucketPolicy, EvictionPolicy::DFS, uint32_t>;
+using XorU64_16_BFS_E16_W32 =
+    CuckooConfig<uint64_t, 16, 16, 256, 16, XorAltBucketPolicy, EvictionPolicy::BFS, uint32_t>;
 
 template <typename Cfg>
 struct Shim {
@@ -89,7 +95,8 @@ const Ops kOps[] = {
     ops_of<XorU64_16_BFS>(),     ops_of<XorU64_16_DFS>(),     ops_of<XorU64_8_BFS>(),
     ops_of<XorU64_8_DFS>(),      ops_of<XorU64_32_BFS>(),     ops_of<XorU64_32_DFS>(),
     ops_of<XorU32_16_DFS>(),     ops_of<XorU64_16_DFS_E16>(), ops_of<XorU64_16_BFS_E16>(),
-    ops_of<XorU64_32_DFS_E16>(), ops_of<XorU64_32_BFS_E16>(),
+    ops_of<XorU64_32_DFS_E16>(), ops_of<XorU64_32_BFS_E16>(), ops_of<XorU64_8_DFS_W32>(),
+    ops_of<XorU64_8_BFS_W32>(),  ops_of<XorU64_16_DFS_W32>(), ops_of<XorU64_16_BFS_E16_W32>(),
 };
 constexpr int kNumOps = sizeof(kOps) / sizeof(kOps[0]);
 
