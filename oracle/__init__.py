@@ -28,6 +28,7 @@ REF_HOST_SO = os.path.join(HERE, "_ref", "libref_host.so")
 REF_GPU_SO = os.path.join(HERE, "_ref", "libref_gpu.so")
 
 POLICY_BFS, POLICY_DFS = 0, 1
+ALT_XOR, ALT_ADDSUB, ALT_OFFSET = 0, 1, 2
 MODE_REFERENCE, MODE_CONSERVING = 0, 1
 STAT_NAMES = ("primary", "secondary", "evicted_inserts", "evictions", "failed")
 
@@ -41,6 +42,7 @@ class Params(C.Structure):
         ("policy", C.c_uint32),
         ("max_evictions", C.c_uint32),
         ("num_buckets", C.c_uint64),
+        ("alt_policy", C.c_uint32),
     ]
 
 
@@ -66,6 +68,10 @@ def lib() -> C.CDLL:
         L.cfo_xxhash64.restype = u64
         L.cfo_num_buckets.argtypes = [u64, u32]
         L.cfo_num_buckets.restype = u64
+        L.cfo_num_buckets_policy.argtypes = [u64, u32, u32]
+        L.cfo_num_buckets_policy.restype = u64
+        L.cfo_alt_tag.argtypes = [P, u32]
+        L.cfo_alt_tag.restype = u32
         L.cfo_alt_bucket.argtypes = [P, u64, u32]
         L.cfo_alt_bucket.restype = u64
         L.cfo_candidates.argtypes = [P, vp, sz, vp, vp, vp]
@@ -103,8 +109,8 @@ def xxhash64(value: int, nbytes: int) -> int:
     return int(lib().cfo_xxhash64(_ptr(b), nbytes))
 
 
-def num_buckets(capacity: int, bucket_size: int) -> int:
-    return int(lib().cfo_num_buckets(capacity, bucket_size))
+def num_buckets(capacity: int, bucket_size: int, alt_policy: int = ALT_XOR) -> int:
+    return int(lib().cfo_num_buckets_policy(capacity, bucket_size, alt_policy))
 
 
 @dataclass
@@ -119,11 +125,12 @@ class OracleFilter:
     max_evictions: int = 500
     capacity: int = 1 << 20
     mode: int = MODE_CONSERVING
+    alt_policy: int = ALT_XOR
 
     def __post_init__(self):
-        self.nb = num_buckets(self.capacity, self.bucket_size)
+        self.nb = num_buckets(self.capacity, self.bucket_size, self.alt_policy)
         self.p = Params(self.key_bytes, self.bits, self.bucket_size, self.word_bytes, self.policy,
-                        self.max_evictions, self.nb)
+                        self.max_evictions, self.nb, self.alt_policy)
         self.bucket_bytes = self.bucket_size * self.bits // 8
         self.table = np.zeros(self.nb * self.bucket_bytes, dtype=np.uint8)
         self.stats = np.zeros(len(STAT_NAMES), dtype=np.uint64)
@@ -145,6 +152,21 @@ class OracleFilter:
 
     def alt_bucket(self, bucket: int, tag: int) -> int:
         return int(lib().cfo_alt_bucket(C.byref(self.p), bucket, tag))
+
+    def alt_tag(self, tag: int) -> int:
+        """The tag as stored in its alternate bucket (Offset policy: choice bit flipped)."""
+        return int(lib().cfo_alt_tag(C.byref(self.p), tag))
+
+    def alt_map(self):
+        """Vectorised (bucket, tag) -> alternate bucket for this filter's policy."""
+        return alt_vectorized(self.bits, self.nb, self.alt_policy)
+
+    def pure_tag(self, tags):
+        """Tags without the Offset policy's choice bit (unchanged otherwise)."""
+        t = np.asarray(tags).astype(np.uint64)
+        if self.alt_policy == ALT_OFFSET:
+            t = t & np.uint64((1 << (self.bits - 1)) - 1)
+        return t
 
     def insert(self, keys, out: bool = False):
         k = self._keys(keys)
@@ -178,7 +200,7 @@ class OracleFilter:
         return self.table.view(dt).reshape(self.nb, self.bucket_size)
 
 
-def check_invariants(slots: np.ndarray, alt_of, keys_i1, keys_i2, keys_fp) -> list[str]:
+def check_invariants(slots: np.ndarray, alt_of, keys_i1, keys_i2, keys_fp, norm=None) -> list[str]:
     """Structural checks on a table image.
 
     ``slots`` is (nb, bs) tags; ``keys_*`` are the candidates of the keys that
@@ -187,17 +209,20 @@ def check_invariants(slots: np.ndarray, alt_of, keys_i1, keys_i2, keys_fp) -> li
       * every stored key's tag sits in one of its two buckets (no false negatives),
       * the multiset {(min(b, alt), max(b, alt), tag)} of stored entries equals the
         multiset of the inserted keys' {(min(i1,i2), max(i1,i2), fp)}.
+    ``norm`` maps tags to the form compared (the Offset policy's tags without
+    their choice bit); identity when None.
     """
+    norm = norm or (lambda x: np.asarray(x).astype(np.uint64))
     errs = []
     b_idx, s_idx = np.nonzero(slots)
     tags = slots[b_idx, s_idx].astype(np.uint64)
     alts = alt_of(b_idx.astype(np.uint64), tags)
     lo = np.minimum(b_idx.astype(np.uint64), alts)
     hi = np.maximum(b_idx.astype(np.uint64), alts)
-    table_set = np.stack([lo, hi, tags], axis=1)
+    table_set = np.stack([lo, hi, norm(tags)], axis=1)
     klo = np.minimum(keys_i1, keys_i2).astype(np.uint64)
     khi = np.maximum(keys_i1, keys_i2).astype(np.uint64)
-    key_set = np.stack([klo, khi, keys_fp.astype(np.uint64)], axis=1)
+    key_set = np.stack([klo, khi, norm(keys_fp)], axis=1)
     if len(table_set) != len(key_set):
         errs.append(f"entry count {len(table_set)} != stored keys {len(key_set)}")
     ts = table_set[np.lexsort(table_set.T[::-1])]
@@ -207,20 +232,39 @@ def check_invariants(slots: np.ndarray, alt_of, keys_i1, keys_i2, keys_fp) -> li
     return errs
 
 
-def alt_vectorized(bits: int, nb: int):
-    """Vectorised alternate-bucket map via a per-tag lookup table."""
+def alt_vectorized(bits: int, nb: int, alt_policy: int = ALT_XOR):
+    """Vectorised alternate-bucket map (per-tag hash lookup table for tags of
+    up to 16 bits) for the XOR, AddSub and Offset policies."""
     ntags = 1 << min(bits, 16)
     if bits <= 16:
-        tbl = np.empty(ntags, np.uint64)
-        for t in range(ntags):
-            tbl[t] = xxhash64(t, bits // 8) & (nb - 1)
+        tbl = np.array([xxhash64(t, bits // 8) for t in range(ntags)], dtype=np.uint64)
+
+        def th(t):
+            return tbl[np.asarray(t).astype(np.int64)]
+    else:
+        def th(t):
+            return np.array([xxhash64(int(x), 4) for x in np.asarray(t)], dtype=np.uint64)
+
+    nbu = np.uint64(nb)
+    if alt_policy == ALT_ADDSUB:
+        half = np.uint64(nb // 2)
 
         def f(b, t):
-            return b ^ tbl[t.astype(np.int64)]
+            b = np.asarray(b).astype(np.uint64)
+            fh = th(t) % half
+            return np.where(b < half, (b + fh) % half + half, (b - fh) % half)
+    elif alt_policy == ALT_OFFSET:
+        cb = np.uint64(1 << (bits - 1))
+
+        def f(b, t):
+            b = np.asarray(b).astype(np.uint64)
+            t = np.asarray(t).astype(np.uint64)
+            off = th(t & (cb - np.uint64(1))) % nbu
+            off = np.where(off == 0, np.uint64(1), off)
+            return np.where((t & cb) == 0, (b + off) % nbu, (b + nbu - off) % nbu)
     else:
         def f(b, t):
-            h = np.array([xxhash64(int(x), 4) & (nb - 1) for x in t], dtype=np.uint64)
-            return b ^ h
+            return np.asarray(b).astype(np.uint64) ^ (th(t) & np.uint64(nb - 1))
     return f
 
 
@@ -241,6 +285,14 @@ def ref_host():
         L.ref_xxhash64.restype = C.c_uint64
         L.ref_num_buckets.argtypes = [C.c_uint64, C.c_uint32]
         L.ref_num_buckets.restype = C.c_uint64
+        L.ref_candidates_policy.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
+                                            C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_candidates_policy.restype = C.c_int
+        L.ref_alt_policy.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_size_t,
+                                     C.c_void_p, C.c_void_p]
+        L.ref_alt_policy.restype = C.c_int
+        L.ref_num_buckets_policy.argtypes = [C.c_uint32, C.c_uint64]
+        L.ref_num_buckets_policy.restype = C.c_uint64
         _ref_host = L
     return _ref_host
 
@@ -343,3 +395,26 @@ class RefGpuFilter:
 
     def num_buckets(self):
         return self.L.refg_num_buckets(self.cfg, self.h)
+
+
+def ref_candidates_policy(alt_policy, key_bytes, bits, nb, keys):
+    """The reference's getCandidateBuckets for an alternate-bucket policy (bucket count nb)."""
+    L = ref_host()
+    k = np.ascontiguousarray(keys, dtype=np.uint64 if key_bytes == 8 else np.uint32)
+    i1 = np.empty(len(k), np.uint64)
+    i2 = np.empty(len(k), np.uint64)
+    fp = np.empty(len(k), np.uint32)
+    rc = L.ref_candidates_policy(alt_policy, key_bytes, bits, nb, _ptr(k), len(k), _ptr(i1), _ptr(i2), _ptr(fp))
+    assert rc == 0
+    return i1, i2, fp
+
+
+def ref_alt_policy(alt_policy, bits, nb, buckets, tags):
+    """The reference's alternate bucket of each (bucket, tag) and the tag as stored there."""
+    L = ref_host()
+    b = np.ascontiguousarray(buckets, dtype=np.uint64)
+    t = np.ascontiguousarray(tags, dtype=np.uint32)
+    alt = np.empty(len(b), np.uint64)
+    nt = np.empty(len(b), np.uint32)
+    assert L.ref_alt_policy(alt_policy, bits, nb, _ptr(b), _ptr(t), len(b), _ptr(alt), _ptr(nt)) == 0
+    return alt, nt

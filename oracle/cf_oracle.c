@@ -13,6 +13,15 @@
  *     branch (:127-158) is reachable; the 32-byte stripe loop is not restated.
  *   - XorAltBucketPolicy: include/bucket_policies.cuh:46-61 (candidates),
  *     :72-74 (alternate bucket), :80-83 (bucket count) + include/helpers.cuh:31-45.
+ *   - AddSubAltBucketPolicy :95-177 (two halves; the alternate of a bucket in
+ *     the first half is (b + h(tag) mod half) mod half + half, of one in the
+ *     second (b - h(tag) mod half) mod half; an even bucket count) and
+ *     OffsetAltBucketPolicy :179-350 (the tag's top bit is a choice bit: 0 in
+ *     the primary bucket, 1 in the alternate; the alternate is b + off or
+ *     b - off mod nB with off = h(tag without the choice bit) mod nB, never 0;
+ *     moving a tag flips its choice bit), as the filter uses them at
+ *     CuckooFilter.cuh:1033-1059 (insert), :1091-1094 (contains),
+ *     :1109-1112 (remove) and :945, :988 (evictions).
  *   - Bucket layout: include/CuckooFilter.cuh:224-237 (slot s of bucket b lives at
  *     byte b*bucketBytes + s*(bits/8), little-endian packed words).
  *   - tryInsertAtBucket :859-904, tryRemoveAtBucket :805-848,
@@ -113,9 +122,49 @@ static inline uint64_t tag_hash(uint32_t tag, uint32_t bits) {
     return cfo_xxhash64(b, bits / 8);
 }
 
-static inline uint64_t alt_bucket(const cfo_params* P, uint64_t b, uint32_t tag) {
-    return b ^ (tag_hash(tag, P->bits) & (P->num_buckets - 1));
+uint64_t cfo_num_buckets_policy(uint64_t capacity, uint32_t bucket_size, uint32_t alt_policy) {
+    if (alt_policy == CFO_ALT_XOR) return cfo_num_buckets(capacity, bucket_size);
+    double req = (double)capacity / (double)bucket_size;
+    uint64_t r = (uint64_t)req;
+    if ((double)r < req) r += 1;
+    if (alt_policy == CFO_ALT_ADDSUB && (r % 2) != 0) r += 1;
+    return r;
 }
+
+static inline uint32_t choice_bit(const cfo_params* P) { return 1u << (P->bits - 1); }
+
+/* Non-zero offset of a tag without its choice bit (computeOffset, :245-249). */
+static inline uint64_t tag_offset(const cfo_params* P, uint32_t pure) {
+    const uint64_t off = tag_hash(pure, P->bits) % P->num_buckets;
+    return off == 0 ? 1 : off;
+}
+
+static inline uint64_t alt_bucket(const cfo_params* P, uint64_t b, uint32_t tag) {
+    const uint64_t nb = P->num_buckets;
+    switch (P->alt_policy) {
+        case CFO_ALT_ADDSUB: {
+            const uint64_t half = nb / 2;
+            const uint64_t fh = tag_hash(tag, P->bits) % half;
+            return b < half ? ((b + fh) % half) + half : (b - fh) % half;
+        }
+        case CFO_ALT_OFFSET: {
+            const uint32_t pure = tag & (choice_bit(P) - 1);
+            const uint64_t off = tag_offset(P, pure);
+            return (tag & choice_bit(P)) == 0 ? (b + off) % nb : (b + nb - off) % nb;
+        }
+        default:
+            return b ^ (tag_hash(tag, P->bits) & (nb - 1));
+    }
+}
+
+/* The tag as stored after it moves to its alternate bucket
+ * (getAlternateBucketWithNewFp, CuckooFilter.cuh:394-401): the Offset
+ * policy flips the choice bit, the others keep the tag. */
+static inline uint32_t alt_tag(const cfo_params* P, uint32_t tag) {
+    return P->alt_policy == CFO_ALT_OFFSET ? (tag ^ choice_bit(P)) : tag;
+}
+
+uint32_t cfo_alt_tag(const cfo_params* P, uint32_t tag) { return alt_tag(P, tag); }
 
 static inline uint64_t key_at(const cfo_params* P, const void* keys, size_t i) {
     if (P->key_bytes == 8) return ((const uint64_t*)keys)[i];
@@ -127,11 +176,16 @@ static inline void candidates(const cfo_params* P, uint64_t key, uint64_t* i1, u
     uint8_t kb[8];
     memcpy(kb, &key, 8);
     const uint64_t h = cfo_xxhash64(kb, P->key_bytes);
-    const uint32_t mask = P->bits == 32 ? 0xFFFFFFFFu : ((1u << P->bits) - 1u);
+    uint32_t mask = P->bits == 32 ? 0xFFFFFFFFu : ((1u << P->bits) - 1u);
+    if (P->alt_policy == CFO_ALT_OFFSET) mask = choice_bit(P) - 1; /* choice bit 0 */
     uint32_t f = (uint32_t)(h >> 32) & mask;
     if (f == 0) f = 1;
     const uint32_t hb = (uint32_t)(h & 0xFFFFFFFFu);
-    *i1 = (uint64_t)hb & (P->num_buckets - 1);
+    switch (P->alt_policy) {
+        case CFO_ALT_ADDSUB: *i1 = (uint64_t)hb % (P->num_buckets / 2); break;
+        case CFO_ALT_OFFSET: *i1 = (uint64_t)hb % P->num_buckets; break;
+        default: *i1 = (uint64_t)hb & (P->num_buckets - 1); break;
+    }
     *i2 = alt_bucket(P, *i1, f);
     *fp = f;
 }
@@ -226,8 +280,8 @@ static int evict_dfs(const cfo_params* P, uint8_t* t, uint32_t fp, uint64_t star
         const uint32_t victim = get_slot(P, t, cb, slot);
         set_slot(P, t, cb, slot, cur);
         if (n_evictions) ++*n_evictions;
-        cur = victim;
         cb = alt_bucket(P, cb, victim);
+        cur = alt_tag(P, victim);
         if (try_insert(P, t, cb, cur)) {
             free(path);
             return 1;
@@ -235,11 +289,12 @@ static int evict_dfs(const cfo_params* P, uint8_t* t, uint32_t fp, uint64_t star
     }
     if (mode == CFO_MODE_CONSERVING) {
         /* Walk back: the held tag returns to the bucket it came from, which
-         * is alt(cb, held) because the alternate map is an involution. */
+         * is alt(cb, held) because the alternate map is an involution (with
+         * the tag in that bucket's form). */
         for (uint32_t e = maxe; e-- > 0;) {
             cb = alt_bucket(P, cb, cur);
             const uint32_t back = get_slot(P, t, cb, path[e]);
-            set_slot(P, t, cb, path[e], cur);
+            set_slot(P, t, cb, path[e], alt_tag(P, cur));
             cur = back;
         }
         /* cur is now fp again and cb == start; fp is discarded. */
@@ -261,35 +316,39 @@ static int evict_bfs(const cfo_params* P, uint8_t* t, uint32_t fp, uint64_t star
             continue;
         }
         const uint64_t alt = alt_bucket(P, start, cand);
-        if (try_insert(P, t, alt, cand)) {
+        if (try_insert(P, t, alt, alt_tag(P, cand))) {
             if (get_slot(P, t, start, slot) == cand) {
                 set_slot(P, t, start, slot, fp);
                 if (n_evictions) ++*n_evictions;
                 return 1;
             }
-            try_remove(P, t, alt, cand);
+            try_remove(P, t, alt, alt_tag(P, cand));
         }
     }
     return evict_dfs(P, t, fp, start, mode, n_evictions);
 }
 
-/* CuckooFilter::insert (CuckooFilter.cuh:1029-1080), Xor policy branch. */
+/* CuckooFilter::insert (CuckooFilter.cuh:1029-1080): the tag goes to its
+ * primary bucket, else (in its alternate form) to its alternate, else eviction
+ * starts at i1 for an even tag and i2 for an odd one. */
 static int insert_one(const cfo_params* P, uint8_t* t, uint64_t key, int mode, uint64_t* stats) {
     uint64_t i1, i2;
     uint32_t fp;
     candidates(P, key, &i1, &i2, &fp);
+    const uint32_t fp2 = alt_tag(P, fp);
     if (try_insert(P, t, i1, fp)) {
         if (stats) stats[CFO_STAT_PRIMARY]++;
         return 1;
     }
-    if (try_insert(P, t, i2, fp)) {
+    if (try_insert(P, t, i2, fp2)) {
         if (stats) stats[CFO_STAT_SECONDARY]++;
         return 1;
     }
     const uint64_t start = (fp & 1) == 0 ? i1 : i2;
+    const uint32_t sfp = (fp & 1) == 0 ? fp : fp2;
     uint64_t ev = 0;
-    int ok = P->policy == CFO_POLICY_BFS ? evict_bfs(P, t, fp, start, mode, &ev)
-                                         : evict_dfs(P, t, fp, start, mode, &ev);
+    int ok = P->policy == CFO_POLICY_BFS ? evict_bfs(P, t, sfp, start, mode, &ev)
+                                         : evict_dfs(P, t, sfp, start, mode, &ev);
     if (stats) {
         stats[CFO_STAT_EVICTED_INSERTS]++;
         stats[CFO_STAT_EVICTIONS] += ev;
@@ -315,7 +374,7 @@ size_t cfo_delete_seq(const cfo_params* P, uint8_t* table, const void* keys, siz
         uint64_t i1, i2;
         uint32_t fp;
         candidates(P, key_at(P, keys, i), &i1, &i2, &fp);
-        int r = try_remove(P, table, i1, fp) || try_remove(P, table, i2, fp);
+        int r = try_remove(P, table, i1, fp) || try_remove(P, table, i2, alt_tag(P, fp));
         if (out) out[i] = (uint8_t)r;
         ok += (size_t)r;
     }
@@ -337,6 +396,7 @@ uint64_t cfo_probe_count(const cfo_params* P, const uint8_t* table, const void* 
         uint64_t i1, i2;
         uint32_t fp;
         candidates(P, key_at(P, keys, i), &i1, &i2, &fp);
+        (void)i2;
         total += bucket_has(P, table, i1, fp) ? 1 : 2;
     }
     return total;
@@ -434,13 +494,13 @@ static int mt_evict_dfs(const cfo_params* P, uint8_t* t, uint32_t fp, uint64_t s
         path[e] = (uint8_t)slot;
         const uint32_t victim = mt_exchange_slot(P, t, cb, slot, cur);
         if (victim == 0) return 1;
-        cur = victim;
         cb = alt_bucket(P, cb, victim);
+        cur = alt_tag(P, victim);
         if (mt_try_insert(P, t, cb, cur)) return 1;
     }
     for (uint32_t e = P->max_evictions; e-- > 0;) {
         cb = alt_bucket(P, cb, cur);
-        cur = mt_exchange_slot(P, t, cb, path[e], cur);
+        cur = mt_exchange_slot(P, t, cb, path[e], alt_tag(P, cur));
         /* A slot emptied concurrently absorbed the held tag: every tag,
          * including fp, is now stored. */
         if (cur == 0) return 1;
@@ -462,13 +522,13 @@ static int mt_evict_bfs(const cfo_params* P, uint8_t* t, uint32_t fp, uint64_t s
             continue;
         }
         const uint64_t alt = alt_bucket(P, start, cand);
-        if (mt_try_insert(P, t, alt, cand)) {
+        if (mt_try_insert(P, t, alt, alt_tag(P, cand))) {
             w = load_word(P, t, start, slot);
             if (((w >> sh) & m) == cand) {
                 const uint64_t d = (w & ~(m << sh)) | ((uint64_t)fp << sh);
                 if (cas_word(P, t, start, slot, &w, d)) return 1;
             }
-            mt_try_remove(P, t, alt, cand);
+            mt_try_remove(P, t, alt, alt_tag(P, cand));
         }
     }
     return mt_evict_dfs(P, t, fp, start, path);
@@ -494,17 +554,19 @@ static void* mt_worker(void* arg) {
         uint32_t fp;
         candidates(P, key_at(P, J->keys, i), &i1, &i2, &fp);
         int r;
+        const uint32_t fp2 = alt_tag(P, fp);
         if (J->op == 0) {
-            r = mt_try_insert(P, J->table, i1, fp) || mt_try_insert(P, J->table, i2, fp);
+            r = mt_try_insert(P, J->table, i1, fp) || mt_try_insert(P, J->table, i2, fp2);
             if (!r) {
                 const uint64_t start = (fp & 1) == 0 ? i1 : i2;
-                r = P->policy == CFO_POLICY_BFS ? mt_evict_bfs(P, J->table, fp, start, path)
-                                                : mt_evict_dfs(P, J->table, fp, start, path);
+                const uint32_t sfp = (fp & 1) == 0 ? fp : fp2;
+                r = P->policy == CFO_POLICY_BFS ? mt_evict_bfs(P, J->table, sfp, start, path)
+                                                : mt_evict_dfs(P, J->table, sfp, start, path);
             }
         } else if (J->op == 1) {
-            r = bucket_has(P, J->table, i1, fp) || bucket_has(P, J->table, i2, fp);
+            r = bucket_has(P, J->table, i1, fp) || bucket_has(P, J->table, i2, fp2);
         } else {
-            r = mt_try_remove(P, J->table, i1, fp) || mt_try_remove(P, J->table, i2, fp);
+            r = mt_try_remove(P, J->table, i1, fp) || mt_try_remove(P, J->table, i2, fp2);
         }
         if (J->out) J->out[i] = (uint8_t)r;
         ok += (size_t)r;

@@ -14,6 +14,8 @@ extern "C" {
 #endif
 
 enum { CFO_POLICY_BFS = 0, CFO_POLICY_DFS = 1 };
+/* Alternate-bucket policy (reference include/bucket_policies.cuh). */
+enum { CFO_ALT_XOR = 0, CFO_ALT_ADDSUB = 1, CFO_ALT_OFFSET = 2 };
 enum { CFO_MODE_REFERENCE = 0, CFO_MODE_CONSERVING = 1 };
 enum {
     CFO_STAT_PRIMARY = 0,
@@ -31,11 +33,14 @@ typedef struct cfo_params {
     uint32_t word_bytes;    /* 4 or 8 */
     uint32_t policy;        /* CFO_POLICY_* */
     uint32_t max_evictions;
-    uint64_t num_buckets;   /* power of two */
+    uint64_t num_buckets;   /* power of two for CFO_ALT_XOR; even for CFO_ALT_ADDSUB */
+    uint32_t alt_policy;    /* CFO_ALT_* */
 } cfo_params;
 
 uint64_t cfo_xxhash64(const void* data, size_t len);
 uint64_t cfo_num_buckets(uint64_t capacity, uint32_t bucket_size);
+uint64_t cfo_num_buckets_policy(uint64_t capacity, uint32_t bucket_size, uint32_t alt_policy);
+uint32_t cfo_alt_tag(const cfo_params* P, uint32_t tag);
 uint64_t cfo_alt_bucket(const cfo_params* P, uint64_t bucket, uint32_t tag);
 void cfo_candidates(const cfo_params* P, const void* keys, size_t n, uint64_t* i1, uint64_t* i2,
                     uint32_t* fp);
