@@ -1002,6 +1002,59 @@ def run_grid(args) -> dict:
                                    "50% positive, 2^26 deletes"}, "rows": rows}
 
 
+# ------------------------------------------------------- alternate-bucket policies
+
+
+def run_policies(args) -> dict:
+    """The three alternate-bucket policies on the large workload's keys
+    (the reference's bucket_policy_benchmark.cu configurations: 16-bit tags,
+    16-slot buckets, DFS): 2^31 slots filled to 0.95 with insertMany, 2^28
+    lookups (50 % positive), 2^26 deletes."""
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    base = dict(WORKLOADS["large"])
+    fill, query, dele, _ = make_inputs(base, dev)
+    q_out = torch.empty(query.numel(), dtype=torch.bool, device=dev)
+    stream = torch.cuda.current_stream()
+    rows = []
+    for name in ("XorAltBucketPolicy", "AddSubAltBucketPolicy", "OffsetAltBucketPolicy"):
+        cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16, bucketSize=16, maxEvictions=500,
+                               evictionPolicy=cfb.EvictionPolicy.DFS, AltBucketPolicy=name)
+        f = cfb.CuckooFilter(cfg, base["capacity"])
+        res = {}
+        for _ in range(2):  # the first pass warms the caches
+            f.clear(stream)
+            f.resetEvictionCount()
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(stream)
+            f.insertManyAsync(fill, stream=stream)
+            e[1].record(stream)
+            f.containsManyAsync(query, q_out, stream=stream)
+            e[2].record(stream)
+            f.deleteManyAsync(dele, stream=stream)
+            e[3].record(stream)
+            torch.cuda.synchronize()
+            st = f.stats()
+            res = {"policy": name, "num_buckets": f.getNumBuckets(), "table_bytes": f.sizeInBytes(),
+                   "insert_gkeys_s": fill.numel() / e[0].elapsed_time(e[1]) / 1e6,
+                   "lookup_gkeys_s": query.numel() / e[1].elapsed_time(e[2]) / 1e6,
+                   "delete_gkeys_s": dele.numel() / e[2].elapsed_time(e[3]) / 1e6,
+                   "failed": st["failed"], "lost": st["lost"], "evictions": st["evictions"],
+                   "lookup_hits": int(q_out.sum().item())}
+        rows.append(res)
+        print(json.dumps(res), file=sys.stderr, flush=True)
+        f.close()
+    return {"form": "policies", "metric": "Gkeys/s per op for each alternate-bucket policy", "unit": "Gkeys/s",
+            "n_gpus": 1, "dtype": "u64", "data": "synthetic: splitmix64 keys (large workload)",
+            "config": {"workload": "2^31 slots, 16/16, DFS, insertMany to 0.95 (2 040 109 465 keys), 2^28 lookups "
+                                   "50% positive, 2^26 deletes"}, "rows": rows}
+
+
 # ------------------------------------------------------------ reference arm
 
 
@@ -1109,7 +1162,7 @@ def main() -> None:
     ap.add_argument("--kmer-file", default=None,
                     help="--form kmer: insert the k-mers of this file (u64 count + u64 2-bit k-mers, the "
                          "reference's k-mer benchmark format) instead of synthetic DNA")
-    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid"), default="plain",
+    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid", "policies"), default="plain",
                     help="batched: the filter-set form over 4096 uneven filters; served: the multi-tenant "
                          "continuous-batching form (each its own JSON line)")
     ap.add_argument("--tenants", type=int, default=256)
@@ -1128,6 +1181,8 @@ def main() -> None:
         res = run_served(args)
     elif args.form == "kmer":
         res = run_kmer(args)
+    elif args.form == "policies":
+        res = run_policies(args)
     elif args.form == "grid":
         res = run_grid(args)
     else:

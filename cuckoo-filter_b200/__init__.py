@@ -104,6 +104,7 @@ def library() -> C.CDLL:
         "cf_status_string": ([i32], C.c_char_p),
         "cf_config_supported": ([C.POINTER(_Config)], i32),
         "cf_num_buckets_for": ([u64, u32], u64),
+        "cf_num_buckets_for_policy": ([u64, u32, u32], u64),
         "cf_create": ([C.POINTER(_Config), u64, PF], i32),
         "cf_destroy": ([vp], i32),
         "cf_get_info": ([vp, C.POINTER(_Info)], i32),
@@ -166,6 +167,10 @@ def _check(status: int) -> None:
 
 _KEY_BYTES = {"uint64": 8, "uint64_t": 8, "int64": 8, "uint32": 4, "uint32_t": 4, "int32": 4}
 
+ALT_XOR, ALT_ADDSUB, ALT_OFFSET = 0, 1, 2
+_ALT_POLICIES = {"XorAltBucketPolicy": ALT_XOR, "xor": ALT_XOR, "AddSubAltBucketPolicy": ALT_ADDSUB,
+                 "addsub": ALT_ADDSUB, "OffsetAltBucketPolicy": ALT_OFFSET, "offset": ALT_OFFSET}
+
 
 @dataclass(frozen=True)
 class CuckooConfig:
@@ -193,12 +198,18 @@ class CuckooConfig:
     def TagType(self) -> str:
         return "uint8_t" if self.bitsPerTag <= 8 else "uint16_t" if self.bitsPerTag <= 16 else "uint32_t"
 
+    @property
+    def alt_policy(self) -> int:
+        """cf_alt_policy of AltBucketPolicy (XorAltBucketPolicy, AddSubAltBucketPolicy or OffsetAltBucketPolicy)."""
+        try:
+            return _ALT_POLICIES[self.AltBucketPolicy]
+        except KeyError:
+            raise CuckooError(-1, f"unknown alternate-bucket policy {self.AltBucketPolicy}") from None
+
     def to_c(self) -> _Config:
-        if self.AltBucketPolicy not in ("XorAltBucketPolicy", "xor"):
-            raise CuckooError(-2, f"alternate-bucket policy {self.AltBucketPolicy} is not built")
         word = {"uint64_t": 8, "uint64": 8, "uint32_t": 4, "uint32": 4}[self.WordType]
         return _Config(self.key_bytes, self.bitsPerTag, self.bucketSize, word, int(self.evictionPolicy),
-                       self.maxEvictions, self.blockSize, 0)
+                       self.maxEvictions, self.blockSize, self.alt_policy)
 
 
 def _torch():
@@ -416,12 +427,14 @@ class CuckooFilter:
 
     # ------------------------------------------------------ static helpers
     @staticmethod
-    def calculateNumBuckets(capacity: int, bucketSize: int = 16) -> int:
-        return int(library().cf_num_buckets_for(capacity, bucketSize))
+    def calculateNumBuckets(capacity: int, bucketSize: int = 16, AltBucketPolicy: str = "XorAltBucketPolicy") -> int:
+        """The policy's calculateNumBuckets (bucket_policies.cuh:80-83, :166-176, :346-349)."""
+        return int(library().cf_num_buckets_for_policy(capacity, bucketSize, _ALT_POLICIES[AltBucketPolicy]))
 
     @staticmethod
     def getCandidateBuckets(config: CuckooConfig, keys, numBuckets: int):
-        """(i1, i2, fp) arrays for host keys (XorAltBucketPolicy::getCandidateBuckets)."""
+        """(i1, i2, fp) arrays for host keys (the configured policy's getCandidateBuckets;
+        fp as stored in the primary bucket)."""
         import numpy as np
 
         k = np.ascontiguousarray(keys, dtype=np.uint64 if config.key_bytes == 8 else np.uint32)

@@ -34,7 +34,7 @@ struct cf_filter {
     int max_grid_aux;
     int sms;
     // segment-staged path
-    bool seg_ok;            // packed (bucket, tag) entries fit in 64 bits
+    bool seg_ok;            // the staged paths apply: XOR policy, packed (bucket, tag) entries fit in 64 bits
     SegGeom geom;
     void* ws;               // workspace (grown on demand, freed with the filter)
     uint64_t ws_bytes;
@@ -89,7 +89,7 @@ const std::vector<OpsTable>& registry() {
 const OpsTable* find_ops(const cf_config* c) {
     for (const OpsTable& o : registry())
         if (o.key_bytes == c->key_bytes && o.bits == c->bits_per_tag && o.bucket_size == c->bucket_size &&
-            o.word_bytes == c->word_bytes)
+            o.word_bytes == c->word_bytes && o.alt_policy == c->alt_policy)
             return &o;
     return nullptr;
 }
@@ -108,10 +108,12 @@ int validate(const cf_config* c) {
         return fail(CF_ERR_INVALID, "max_evictions must be in [1, %u]", kMaxEvictionsCap);
     if (c->block_size != 0 && (c->block_size % 32 != 0 || c->block_size > 512))
         return fail(CF_ERR_INVALID, "block_size must be 0 or a multiple of 32 up to 512");
-    if (c->alt_policy != CF_ALT_XOR) return fail(CF_ERR_UNSUPPORTED, "only the XOR alternate-bucket policy is built");
+    if (c->alt_policy != CF_ALT_XOR && c->alt_policy != CF_ALT_ADDSUB && c->alt_policy != CF_ALT_OFFSET)
+        return fail(CF_ERR_INVALID, "alt_policy must be CF_ALT_XOR, CF_ALT_ADDSUB or CF_ALT_OFFSET");
     if (!find_ops(c))
-        return fail(CF_ERR_UNSUPPORTED, "no kernels for key_bytes=%u bits_per_tag=%u bucket_size=%u word_bytes=%u",
-                    c->key_bytes, c->bits_per_tag, c->bucket_size, c->word_bytes);
+        return fail(CF_ERR_UNSUPPORTED,
+                    "no kernels for key_bytes=%u bits_per_tag=%u bucket_size=%u word_bytes=%u alt_policy=%u",
+                    c->key_bytes, c->bits_per_tag, c->bucket_size, c->word_bytes, c->alt_policy);
     return CF_OK;
 }
 
@@ -128,6 +130,14 @@ uint64_t num_buckets_for(uint64_t capacity, uint32_t bucket_size) {
     n |= n >> 16;
     n |= n >> 32;
     return n + 1;
+}
+
+// calculateNumBuckets of each policy (bucket_policies.cuh:80-83, :166-176, :346-349).
+uint64_t num_buckets_policy(uint64_t capacity, uint32_t bucket_size, uint32_t alt_policy) {
+    if (alt_policy == CF_ALT_XOR) return num_buckets_for(capacity, bucket_size);
+    uint64_t r = static_cast<uint64_t>(std::ceil(static_cast<double>(capacity) / static_cast<double>(bucket_size)));
+    if (alt_policy == CF_ALT_ADDSUB && (r % 2) != 0) r += 1;
+    return r;
 }
 
 DevTable dev(const cf_filter* f) {
@@ -193,8 +203,10 @@ void init_geometry(cf_filter* f) {
     f->geom.seg_shift = static_cast<int>(f->cfg.bits_per_tag) + f->geom.sb_log2;
     const int seg_bits = f->geom.nseg > 1 ? ilog2(f->geom.nseg) : 0;
     f->geom.passes = seg_bits == 0 ? 1 : (seg_bits + kRadixBits - 1) / kRadixBits;
-    // (bucket << bits) | tag must fit in 64 bits for every bucket index
-    f->seg_ok = ilog2(f->num_buckets) + static_cast<int>(f->cfg.bits_per_tag) <= 64;
+    // (bucket << bits) | tag must fit in 64 bits for every bucket index, and
+    // the staged paths exist for the XOR policy only
+    f->seg_ok = ilog2(f->num_buckets) + static_cast<int>(f->cfg.bits_per_tag) <= 64 && f->ops->seg_chunk &&
+                f->ops->rg_chunk;
     // regions of ~kRgRegionBytes (or CF_OPT_REGION_BYTES), at most kRgMaxRegions of them
     const int nb_log2 = ilog2(f->num_buckets);
     const uint64_t rbytes = f->rg_bytes ? f->rg_bytes : kRgRegionBytes;
@@ -380,17 +392,25 @@ void host_candidates_t(uint64_t mask, const void* keys, uint64_t n, uint64_t* i1
 }
 
 // Bucket size does not enter the hashing; 16 slots stands in for any.
-void host_candidates(uint32_t kb, uint32_t bits, uint64_t mask, const void* keys, uint64_t n, uint64_t* i1,
-                     uint64_t* i2, uint32_t* fp) {
+template <int POL>
+void host_candidates_p(uint32_t kb, uint32_t bits, uint64_t nbm, const void* keys, uint64_t n, uint64_t* i1,
+                       uint64_t* i2, uint32_t* fp) {
     if (kb == 8) {
-        if (bits == 8) host_candidates_t<Cfg<8, 8, 16, 8>>(mask, keys, n, i1, i2, fp);
-        else if (bits == 16) host_candidates_t<Cfg<8, 16, 16, 8>>(mask, keys, n, i1, i2, fp);
-        else host_candidates_t<Cfg<8, 32, 8, 8>>(mask, keys, n, i1, i2, fp);
+        if (bits == 8) host_candidates_t<Cfg<8, 8, 16, 8, POL>>(nbm, keys, n, i1, i2, fp);
+        else if (bits == 16) host_candidates_t<Cfg<8, 16, 16, 8, POL>>(nbm, keys, n, i1, i2, fp);
+        else host_candidates_t<Cfg<8, 32, 8, 8, POL>>(nbm, keys, n, i1, i2, fp);
     } else {
-        if (bits == 8) host_candidates_t<Cfg<4, 8, 16, 8>>(mask, keys, n, i1, i2, fp);
-        else if (bits == 16) host_candidates_t<Cfg<4, 16, 16, 8>>(mask, keys, n, i1, i2, fp);
-        else host_candidates_t<Cfg<4, 32, 8, 8>>(mask, keys, n, i1, i2, fp);
+        if (bits == 8) host_candidates_t<Cfg<4, 8, 16, 8, POL>>(nbm, keys, n, i1, i2, fp);
+        else if (bits == 16) host_candidates_t<Cfg<4, 16, 16, 8, POL>>(nbm, keys, n, i1, i2, fp);
+        else host_candidates_t<Cfg<4, 32, 8, 8, POL>>(nbm, keys, n, i1, i2, fp);
     }
+}
+
+void host_candidates(uint32_t pol, uint32_t kb, uint32_t bits, uint64_t nbm, const void* keys, uint64_t n,
+                     uint64_t* i1, uint64_t* i2, uint32_t* fp) {
+    if (pol == CF_ALT_ADDSUB) host_candidates_p<ALT_ADDSUB>(kb, bits, nbm, keys, n, i1, i2, fp);
+    else if (pol == CF_ALT_OFFSET) host_candidates_p<ALT_OFFSET>(kb, bits, nbm, keys, n, i1, i2, fp);
+    else host_candidates_p<ALT_XOR>(kb, bits, nbm, keys, n, i1, i2, fp);
 }
 
 }  // namespace
@@ -431,6 +451,11 @@ uint64_t cf_num_buckets_for(uint64_t capacity, uint32_t bucket_size) {
     return num_buckets_for(capacity, bucket_size);
 }
 
+uint64_t cf_num_buckets_for_policy(uint64_t capacity, uint32_t bucket_size, uint32_t alt_policy) {
+    if (bucket_size == 0 || alt_policy > CF_ALT_OFFSET) return 0;
+    return num_buckets_policy(capacity, bucket_size, alt_policy);
+}
+
 int cf_create(const cf_config* cfg, uint64_t capacity, cf_filter** out) {
     if (!out) return fail(CF_ERR_INVALID, "out is NULL");
     *out = nullptr;
@@ -445,7 +470,7 @@ int cf_create(const cf_config* cfg, uint64_t capacity, cf_filter** out) {
     f->cfg = *cfg;
     f->ops = find_ops(cfg);
     f->device = device;
-    f->num_buckets = num_buckets_for(capacity, cfg->bucket_size);
+    f->num_buckets = num_buckets_policy(capacity, cfg->bucket_size, cfg->alt_policy);
     f->table_bytes = f->num_buckets * f->ops->bucket_bytes;
     f->block = cfg->block_size ? static_cast<int>(cfg->block_size) : 256;
     int sms = 0;
@@ -739,13 +764,17 @@ int cf_store_table(cf_filter* f, void* dst, uint64_t bytes, void* stream) {
 int cf_hash_candidates(const cf_config* cfg, uint64_t num_buckets, const void* h_keys, uint64_t n, uint64_t* i1,
                        uint64_t* i2, uint32_t* fp) {
     if (!cfg) return fail(CF_ERR_INVALID, "config is NULL");
-    if (num_buckets == 0 || (num_buckets & (num_buckets - 1)))
-        return fail(CF_ERR_INVALID, "num_buckets must be a power of two");
+    const uint32_t pol = cfg->alt_policy;
+    if (pol > CF_ALT_OFFSET) return fail(CF_ERR_INVALID, "alt_policy must be CF_ALT_XOR, CF_ALT_ADDSUB or CF_ALT_OFFSET");
+    if (num_buckets == 0 || (pol == CF_ALT_XOR && (num_buckets & (num_buckets - 1))))
+        return fail(CF_ERR_INVALID, "num_buckets must be a power of two for the XOR policy, > 0 otherwise");
+    if (pol == CF_ALT_ADDSUB && num_buckets % 2 != 0)
+        return fail(CF_ERR_INVALID, "num_buckets must be even for the AddSub policy");
     if (n && !h_keys) return fail(CF_ERR_INVALID, "keys is NULL with n > 0");
     const uint32_t kb = cfg->key_bytes, bits = cfg->bits_per_tag;
     if ((kb != 4 && kb != 8) || (bits != 8 && bits != 16 && bits != 32))
         return fail(CF_ERR_INVALID, "key_bytes must be 4/8 and bits_per_tag 8/16/32");
-    host_candidates(kb, bits, num_buckets - 1, h_keys, n, i1, i2, fp);
+    host_candidates(pol, kb, bits, num_buckets - 1, h_keys, n, i1, i2, fp);
     return CF_OK;
 }
 
@@ -768,16 +797,32 @@ int cf_hash64(uint32_t value_bytes, const void* h_values, uint64_t n, uint64_t* 
 int cf_alt_buckets(const cf_config* cfg, uint64_t num_buckets, const uint64_t* buckets, const uint32_t* tags,
                    uint64_t n, uint64_t* out) {
     if (!cfg) return fail(CF_ERR_INVALID, "config is NULL");
-    if (num_buckets == 0 || (num_buckets & (num_buckets - 1)))
-        return fail(CF_ERR_INVALID, "num_buckets must be a power of two");
+    const uint32_t pol = cfg->alt_policy;
+    if (pol > CF_ALT_OFFSET) return fail(CF_ERR_INVALID, "alt_policy must be CF_ALT_XOR, CF_ALT_ADDSUB or CF_ALT_OFFSET");
+    if (num_buckets == 0 || (pol == CF_ALT_XOR && (num_buckets & (num_buckets - 1))))
+        return fail(CF_ERR_INVALID, "num_buckets must be a power of two for the XOR policy, > 0 otherwise");
+    if (pol == CF_ALT_ADDSUB && num_buckets % 2 != 0)
+        return fail(CF_ERR_INVALID, "num_buckets must be even for the AddSub policy");
     if (n && (!buckets || !tags || !out)) return fail(CF_ERR_INVALID, "buckets, tags or out is NULL with n > 0");
     const uint32_t bits = cfg->bits_per_tag;
     if (bits != 8 && bits != 16 && bits != 32) return fail(CF_ERR_INVALID, "bits_per_tag must be 8, 16 or 32");
-    const uint64_t mask = num_buckets - 1;
+    const uint64_t nbm = num_buckets - 1;
     for (uint64_t i = 0; i < n; ++i) {
         const uint32_t t = bits == 32 ? tags[i] : (tags[i] & ((1u << bits) - 1u));
-        const uint64_t h = bits == 8 ? xxh64_u8(t) : bits == 16 ? xxh64_u16(t) : xxh64_u32(t);
-        out[i] = buckets[i] ^ (h & mask);
+        uint64_t a;
+#define CF_ALT_CASE(B)                                                                   \
+    if (pol == CF_ALT_ADDSUB) a = alt_bucket<Cfg<8, B, 16, 8, ALT_ADDSUB>>(buckets[i], t, nbm); \
+    else if (pol == CF_ALT_OFFSET) a = alt_bucket<Cfg<8, B, 16, 8, ALT_OFFSET>>(buckets[i], t, nbm); \
+    else a = alt_bucket<Cfg<8, B, 16, 8>>(buckets[i], t, nbm);
+        if (bits == 8) {
+            CF_ALT_CASE(8)
+        } else if (bits == 16) {
+            CF_ALT_CASE(16)
+        } else {
+            CF_ALT_CASE(32)
+        }
+#undef CF_ALT_CASE
+        out[i] = a;
     }
     return CF_OK;
 }
@@ -868,7 +913,8 @@ int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8
         return fail(CF_ERR_INVALID, "%llu keys exceed the %llu-key limit of cf_insert_sorted_noalloc; split the batch",
                     static_cast<unsigned long long>(n), static_cast<unsigned long long>(kNoAllocMaxKeys));
     if (!f->seg_ok)
-        return fail(CF_ERR_UNSUPPORTED, "bucket index and tag do not fit one 64-bit entry for this table");
+        return fail(CF_ERR_UNSUPPORTED, "the segment-staged path does not apply to this table (alternate-bucket "
+                                        "policy other than XOR, or bucket index and tag wider than 64 bits)");
     if (f->geom.nseg > kNoAllocMaxSegments)
         return fail(CF_ERR_UNSUPPORTED, "table of %llu segments exceeds the %llu-segment limit of the fixed scratch",
                     static_cast<unsigned long long>(f->geom.nseg), static_cast<unsigned long long>(kNoAllocMaxSegments));

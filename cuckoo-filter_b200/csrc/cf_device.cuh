@@ -97,8 +97,18 @@ __host__ __device__ __forceinline__ uint64_t hash_tag(uint32_t tag) {
 
 // KB = key bytes (4/8), BITS = tag bits (8/16/32), BS = slots per bucket,
 // WB = CAS word bytes (8; the reference's WordType).
-template <int KB, int BITS, int BS, int WB>
+// Alternate-bucket policy (reference include/bucket_policies.cuh): XOR (:15-84),
+// AddSub (:95-177), Offset (:179-350).
+constexpr int ALT_XOR = 0;
+constexpr int ALT_ADDSUB = 1;
+constexpr int ALT_OFFSET = 2;
+
+template <int KB, int BITS, int BS, int WB, int POL = ALT_XOR>
 struct Cfg {
+    static constexpr int alt_policy = POL;
+    // The Offset policy keeps a choice bit in the tag's top bit: 0 while the tag
+    // is in its primary bucket, 1 in its alternate.
+    static constexpr uint32_t choice_bit = POL == ALT_OFFSET ? (1u << (BITS - 1)) : 0u;
     static constexpr int key_bytes = KB;
     static constexpr int bits = BITS;
     static constexpr int bs = BS;
@@ -120,21 +130,58 @@ struct Cfg {
     static_assert(BITS <= WB * 8, "a tag must fit in one word");
     static_assert(BS % tpw == 0, "bucket size must be a multiple of tags per word");
     static_assert(BS <= 64, "at most 64 slots per bucket");
+    static_assert(POL == ALT_XOR || POL == ALT_ADDSUB || POL == ALT_OFFSET, "alternate-bucket policy");
     using Key = typename std::conditional<KB == 8, uint64_t, uint32_t>::type;
 };
 
-// Bucket derivation (XorAltBucketPolicy::getCandidateBuckets).
+// Bucket derivation (getCandidateBuckets of the configured policy).
+// `nbm` is the bucket count minus one: the index mask of the XOR policy, whose
+// bucket count is a power of two; AddSub and Offset take any (even, for
+// AddSub) bucket count and reduce modulo it.
 template <class C>
-__host__ __device__ __forceinline__ void candidates(uint64_t key, uint64_t nb_mask, uint64_t& i1, uint32_t& fp) {
+__host__ __device__ __forceinline__ void candidates(uint64_t key, uint64_t nbm, uint64_t& i1, uint32_t& fp) {
     const uint64_t h = hash_key<C::key_bytes>(key);
-    uint32_t f = static_cast<uint32_t>(h >> 32) & C::tag_mask;
-    fp = f == 0 ? 1u : f;
-    i1 = static_cast<uint64_t>(static_cast<uint32_t>(h)) & nb_mask;
+    const uint32_t hb = static_cast<uint32_t>(h);
+    if constexpr (C::alt_policy == ALT_OFFSET) {
+        // (bitsPerTag - 1) fingerprint bits, choice bit 0 (:232-247)
+        const uint32_t f = static_cast<uint32_t>(h >> 32) & (C::choice_bit - 1u);
+        fp = f == 0 ? 1u : f;
+        i1 = static_cast<uint64_t>(hb) % (nbm + 1);
+    } else {
+        const uint32_t f = static_cast<uint32_t>(h >> 32) & C::tag_mask;
+        fp = f == 0 ? 1u : f;
+        if constexpr (C::alt_policy == ALT_ADDSUB)
+            i1 = static_cast<uint64_t>(hb) % ((nbm + 1) / 2);  // first half (:128-137)
+        else
+            i1 = static_cast<uint64_t>(hb) & nbm;
+    }
 }
 
+// The other bucket of a tag stored in bucket b (getAlternateBucket).
 template <class C>
-__host__ __device__ __forceinline__ uint64_t alt_bucket(uint64_t b, uint32_t tag, uint64_t nb_mask) {
-    return b ^ (hash_tag<C::bits>(tag) & nb_mask);
+__host__ __device__ __forceinline__ uint64_t alt_bucket(uint64_t b, uint32_t tag, uint64_t nbm) {
+    if constexpr (C::alt_policy == ALT_ADDSUB) {
+        // first half -> second by adding, second -> first by subtracting (:150-160)
+        const uint64_t half = (nbm + 1) / 2;
+        const uint64_t fh = hash_tag<C::bits>(tag) % half;
+        return b < half ? ((b + fh) % half) + half : (b - fh) % half;
+    } else if constexpr (C::alt_policy == ALT_OFFSET) {
+        // +offset from the primary, -offset from the alternate (:300-323)
+        const uint64_t nb = nbm + 1;
+        uint64_t off = hash_tag<C::bits>(tag & (C::choice_bit - 1u)) % nb;
+        off = off == 0 ? 1 : off;
+        return (tag & C::choice_bit) == 0 ? (b + off) % nb : (b + nb - off) % nb;
+    } else {
+        return b ^ (hash_tag<C::bits>(tag) & nbm);
+    }
+}
+
+// The tag as stored once it moves to its other bucket
+// (getAlternateBucketWithNewFp, CuckooFilter.cuh:394-401): the Offset policy
+// flips the choice bit; XOR and AddSub keep the tag.
+template <class C>
+__host__ __device__ __forceinline__ uint32_t alt_tag(uint32_t tag) {
+    return tag ^ C::choice_bit;
 }
 
 // ------------------------------------------------------------------- SWAR

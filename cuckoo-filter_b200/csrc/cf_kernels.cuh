@@ -278,20 +278,23 @@ struct EvictStats {
 };
 
 // Undo of a BFS copy (reference CuckooFilter.cuh:1011-1012): remove one instance
-// of `tag` from its bucket pair {a, b}.  While the copy was in place another
-// walk may have moved it to the other bucket of the pair, or be carrying an
-// instance between the two, so both buckets are tried, a bounded number of
-// times.  Any instance will do: equal tags of one pair are interchangeable.
+// of a tag from its bucket pair {a, b}, where it is stored as `tag_a` in a and
+// as alt_tag(tag_a) in b.  While the copy was in place another walk may have
+// moved it to the other bucket of the pair, or be carrying an instance between
+// the two, so both buckets are tried, a bounded number of times.  Any instance
+// will do: equal tags of one pair are interchangeable.  (The reference removes
+// the candidate's old form from the alternate bucket; under the Offset policy
+// that is not the form it copied there.)
 template <class C>
-__device__ bool remove_from_pair(const DevTable& t, uint64_t a, uint64_t b, uint32_t tag, bool& err) {
+__device__ bool remove_from_pair(const DevTable& t, uint64_t a, uint64_t b, uint32_t tag_a, bool& err) {
     for (int it = 0; it < 1024; ++it) {
         uint64_t c[C::nchunks];
         uint64_t* aw = bucket_words<C>(t, a);
         load_rlx<C::bucket_bytes>(aw, c);
-        if (try_remove<C>(aw, c, tag, err)) return true;
+        if (try_remove<C>(aw, c, tag_a, err)) return true;
         uint64_t* bw = bucket_words<C>(t, b);
         load_rlx<C::bucket_bytes>(bw, c);
-        if (try_remove<C>(bw, c, tag, err)) return true;
+        if (try_remove<C>(bw, c, alt_tag<C>(tag_a), err)) return true;
         if (err) return false;
         __nanosleep(100);
     }
@@ -312,8 +315,8 @@ __device__ __noinline__ bool evict_dfs(DevTable t, uint32_t fp, uint64_t start, 
         if (err) return false;
         ++st.evictions;
         if (victim == 0) return true;  // a slot emptied concurrently took the tag
-        cur = victim;
         cb = alt_bucket<C>(cb, victim, t.nb_mask);
+        cur = alt_tag<C>(victim);
         uint64_t c[C::nchunks];
         uint64_t* bw = bucket_words<C>(t, cb);
         load_rlx<C::bucket_bytes>(bw, c);
@@ -321,10 +324,11 @@ __device__ __noinline__ bool evict_dfs(DevTable t, uint32_t fp, uint64_t start, 
         if (err) return false;
     }
     // Out of evictions: walk the chain back.  The held tag returns to the
-    // bucket it was taken from, alt(cb, held), at the logged slot.
+    // bucket it was taken from, alt(cb, held), at the logged slot (in that
+    // bucket's form).
     for (uint32_t e = max_ev; e-- > 0;) {
         cb = alt_bucket<C>(cb, cur, t.nb_mask);
-        cur = exchange_slot<C>(bucket_words<C>(t, cb), path[e], cur, err);
+        cur = exchange_slot<C>(bucket_words<C>(t, cb), path[e], alt_tag<C>(cur), err);
         if (err) return false;
         if (cur == 0) return true;
     }
@@ -339,7 +343,7 @@ __device__ __noinline__ bool evict_dfs(DevTable t, uint32_t fp, uint64_t start, 
         const uint64_t ab = alt_bucket<C>(cb, cur, t.nb_mask);
         bw = bucket_words<C>(t, ab);
         load_rlx<C::bucket_bytes>(bw, c);
-        if (try_insert<C>(bw, c, cur, err)) return true;
+        if (try_insert<C>(bw, c, alt_tag<C>(cur), err)) return true;
     }
     ++st.lost;
     return true;
@@ -375,7 +379,7 @@ __device__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, uint64_t othe
         const uint64_t ab = alt_bucket<C>(start, cand, t.nb_mask);
         uint64_t* abw = bucket_words<C>(t, ab);
         load_rlx<C::bucket_bytes>(abw, c);
-        if (try_insert<C>(abw, c, cand, err)) {
+        if (try_insert<C>(abw, c, alt_tag<C>(cand), err)) {
             word = load_word_rlx(sbw + w);
             if (((word >> sh) & lane_mask) == cand) {
                 const uint64_t desired = (word & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
@@ -384,7 +388,7 @@ __device__ bool evict_bfs(DevTable t, uint32_t fp, uint64_t start, uint64_t othe
                     return true;
                 }
             }
-            if (!remove_from_pair<C>(t, ab, start, cand, err)) ++st.dup;
+            if (!remove_from_pair<C>(t, ab, start, alt_tag<C>(cand), err)) ++st.dup;
             load_rlx<C::bucket_bytes>(sbw, snap);  // the start bucket changed under us
         }
         if (err) return false;
@@ -495,7 +499,7 @@ __global__ void __launch_bounds__(512) k_contains(DevTable t, const typename C::
         }
 #pragma unroll
         for (int j = 0; j < KPT; ++j)
-            if (k0 + j < n && !((hit >> j) & 1u) && has_tag<C>(c[j], fp[j])) hit |= 1u << j;
+            if (k0 + j < n && !((hit >> j) & 1u) && has_tag<C>(c[j], alt_tag<C>(fp[j]))) hit |= 1u << j;
         store_results<KPT>(out, k0, n, out_vec, hit);
     }
 }
@@ -532,7 +536,8 @@ __global__ void __launch_bounds__(512) k_delete(DevTable t, const typename C::Ke
         }
 #pragma unroll
         for (int j = 0; j < KPT; ++j)
-            if (k0 + j < n && !((done >> j) & 1u) && try_remove<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err))
+            if (k0 + j < n && !((done >> j) & 1u) &&
+                try_remove<C>(bucket_words<C>(t, b[j]), c[j], alt_tag<C>(fp[j]), err))
                 done |= 1u << j;
         removed += __popc(done);
         if (out) store_results<KPT>(out, k0, n, out_vec, done);
@@ -556,9 +561,10 @@ __device__ __noinline__ bool evict_key(DevTable t, uint64_t key, uint32_t policy
     const uint64_t i2 = alt_bucket<C>(i1, fp, t.nb_mask);
     const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
     const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
+    const uint32_t sfp = (fp & 1u) == 0 ? fp : alt_tag<C>(fp);  // the tag in the start bucket's form
     const uint32_t before = st.evictions;
-    const bool ok = policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
-                               : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+    const bool ok = policy_bfs ? evict_bfs<C>(t, sfp, start, other, max_ev, st, err)
+                               : evict_dfs<C>(t, sfp, start, other, max_ev, st, err);
     if (ok) record_chain(t, st.evictions - before);
     return ok;
 }
@@ -636,7 +642,7 @@ __global__ void __launch_bounds__(512) k_insert(DevTable t, const typename C::Ke
                 uint32_t sec = 0;
 #pragma unroll
                 for (int j = 0; j < KPT; ++j)
-                    if (((miss >> j) & 1u) && try_insert<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err))
+                    if (((miss >> j) & 1u) && try_insert<C>(bucket_words<C>(t, b[j]), c[j], alt_tag<C>(fp[j]), err))
                         sec |= 1u << j;
                 n_sec += __popc(sec);
                 done |= sec;

@@ -79,7 +79,7 @@ struct LaunchCfg {
 };
 
 struct OpsTable {
-    uint32_t key_bytes, bits, bucket_size, word_bytes;
+    uint32_t key_bytes, bits, bucket_size, word_bytes, alt_policy;
     uint32_t bucket_bytes;
     int kpt[KID_COUNT_KERNELS];
     cudaError_t (*contains)(const DevTable&, const void*, uint64_t, uint8_t*, const LaunchCfg&);
@@ -477,6 +477,7 @@ struct Launchers {
         o.bits = C::bits;
         o.bucket_size = C::bs;
         o.word_bytes = C::word_bytes;
+        o.alt_policy = C::alt_policy;
         o.bucket_bytes = C::bucket_bytes;
         o.kpt[KID_CONTAINS] = kContainsKPT;
         o.kpt[KID_DELETE] = kDeleteKPT;
@@ -487,8 +488,12 @@ struct Launchers {
         o.count = count;
         o.probe = probe;
         o.occupancy = occupancy;
-        o.seg_chunk = seg_chunk;
-        o.rg_chunk = rg_chunk;
+        // the staged paths sort packed (bucket, tag) entries by the XOR
+        // policy's power-of-two bucket index; other policies probe at random
+        if constexpr (C::alt_policy == ALT_XOR) {
+            o.seg_chunk = seg_chunk;
+            o.rg_chunk = rg_chunk;
+        }
         return o;
     }
 };

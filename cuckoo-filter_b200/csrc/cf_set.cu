@@ -168,7 +168,7 @@ const std::vector<SetOps>& set_registry() {
 }
 
 const SetOps* find_set_ops(const cf_config* c) {
-    if (c->key_bytes != 8 || c->word_bytes != 8) return nullptr;
+    if (c->key_bytes != 8 || c->word_bytes != 8 || c->alt_policy != CF_ALT_XOR) return nullptr;
     for (const SetOps& o : set_registry())
         if (o.bits == c->bits_per_tag && o.bucket_size == c->bucket_size) return &o;
     return nullptr;

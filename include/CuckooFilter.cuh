@@ -79,17 +79,13 @@ inline void candidates(const cf_config& cfg, std::uint64_t num_buckets, const vo
 
 }  // namespace cuckoo_b200
 
-/*
- * XOR alternate-bucket policy (reference bucket_policies.cuh:15-84): tag from
- * the upper 32 bits of xxHash64(key) (0 maps to 1), primary bucket from the
- * lower 32 bits, alternate bucket = bucket ^ (xxHash64(tag) & (numBuckets - 1)),
- * numBuckets = nextPowerOfTwo(ceil(capacity / bucketSize)).  The static
- * functions are evaluated on the host by the library, with the same code the
- * kernels use.
- */
-template <typename KeyType, typename TagType, std::size_t bitsPerTag, std::size_t bucketSize>
-struct XorAltBucketPolicy {
-    static constexpr bool usesChoiceBit = false;
+namespace cuckoo_b200 {
+
+/* Host-side functions shared by the alternate-bucket policies: evaluated by
+ * the library with the same code the kernels use. */
+template <typename KeyType, typename TagType, std::size_t bitsPerTag, std::size_t bucketSize, cf_alt_policy ALT>
+struct AltPolicyBase {
+    static constexpr cf_alt_policy alt_policy = ALT;
 
     static cf_config config() {
         cf_config c{};
@@ -100,31 +96,93 @@ struct XorAltBucketPolicy {
         c.eviction_policy = CF_EVICT_DFS;
         c.max_evictions = 500;
         c.block_size = 0;
-        c.alt_policy = CF_ALT_XOR;
+        c.alt_policy = ALT;
         return c;
     }
 
+    /* (i1, i2, fp): fp as stored in the primary bucket i1. */
     static std::tuple<std::size_t, std::size_t, TagType> getCandidateBuckets(const KeyType& key,
                                                                             std::size_t numBuckets) {
         std::uint64_t i1 = 0, i2 = 0;
         std::uint32_t fp = 0;
         const cf_config c = config();
-        cuckoo_b200::candidates(c, numBuckets, &key, &i1, &i2, &fp);
+        candidates(c, numBuckets, &key, &i1, &i2, &fp);
         return {static_cast<std::size_t>(i1), static_cast<std::size_t>(i2), static_cast<TagType>(fp)};
     }
 
-    /* getAlternateBucket (:72-74): bucket ^ (xxHash64(fp) & (numBuckets - 1)). */
     static std::size_t getAlternateBucket(std::size_t bucket, TagType fp, std::size_t numBuckets) {
         const cf_config c = config();
         const std::uint64_t b = bucket;
         const std::uint32_t t = fp;
         std::uint64_t out = 0;
-        cuckoo_b200::check(cf_alt_buckets(&c, numBuckets, &b, &t, 1, &out), "cf_alt_buckets");
+        check(cf_alt_buckets(&c, numBuckets, &b, &t, 1, &out), "cf_alt_buckets");
         return static_cast<std::size_t>(out);
     }
 
     static std::size_t calculateNumBuckets(std::size_t capacity) {
-        return static_cast<std::size_t>(cf_num_buckets_for(capacity, static_cast<std::uint32_t>(bucketSize)));
+        return static_cast<std::size_t>(
+            cf_num_buckets_for_policy(capacity, static_cast<std::uint32_t>(bucketSize), ALT));
+    }
+};
+
+}  // namespace cuckoo_b200
+
+/*
+ * XOR alternate-bucket policy (reference bucket_policies.cuh:15-84): tag from
+ * the upper 32 bits of xxHash64(key) (0 maps to 1), primary bucket from the
+ * lower 32 bits, alternate bucket = bucket ^ (xxHash64(tag) & (numBuckets - 1)),
+ * numBuckets = nextPowerOfTwo(ceil(capacity / bucketSize)).
+ */
+template <typename KeyType, typename TagType, std::size_t bitsPerTag, std::size_t bucketSize>
+struct XorAltBucketPolicy
+    : cuckoo_b200::AltPolicyBase<KeyType, TagType, bitsPerTag, bucketSize, CF_ALT_XOR> {
+    static constexpr bool usesChoiceBit = false;
+    static constexpr char name[] = "XorAltBucketPolicy";
+};
+
+/*
+ * Additive/subtractive policy (reference bucket_policies.cuh:95-177): the
+ * table is two halves; a key's primary bucket is in the first half (lower 32
+ * hash bits mod numBuckets/2), its alternate in the second:
+ * (bucket + h(tag) mod half) mod half + half, and back by subtracting.
+ * numBuckets = ceil(capacity / bucketSize) rounded up to even.
+ */
+template <typename KeyType, typename TagType, std::size_t bitsPerTag, std::size_t bucketSize>
+struct AddSubAltBucketPolicy
+    : cuckoo_b200::AltPolicyBase<KeyType, TagType, bitsPerTag, bucketSize, CF_ALT_ADDSUB> {
+    static constexpr bool usesChoiceBit = false;
+    static constexpr char name[] = "AddSubAltBucketPolicy";
+};
+
+/*
+ * Offset policy with a choice bit (reference bucket_policies.cuh:179-350): the
+ * tag's top bit is 0 in the primary bucket and 1 in the alternate; the
+ * alternate is (bucket + off) mod numBuckets from the primary and
+ * (bucket - off) mod numBuckets back, off = h(tag without the bit) mod
+ * numBuckets (0 maps to 1).  Any numBuckets = ceil(capacity / bucketSize).
+ */
+template <typename KeyType, typename TagType, std::size_t bitsPerTag, std::size_t bucketSize>
+struct OffsetAltBucketPolicy
+    : cuckoo_b200::AltPolicyBase<KeyType, TagType, bitsPerTag, bucketSize, CF_ALT_OFFSET> {
+    static_assert(bitsPerTag >= 2, "bitsPerTag must be at least 2 for choice bit");
+    static constexpr bool usesChoiceBit = true;
+    static constexpr char name[] = "OffsetAltBucketPolicy";
+    static constexpr std::size_t choiceBitPos = bitsPerTag - 1;
+    static constexpr TagType choiceBitMask = TagType(TagType(1) << choiceBitPos);
+    static constexpr TagType pureFpMask = TagType(choiceBitMask - 1);
+
+    static TagType getPureFingerprint(TagType fp) { return fp & pureFpMask; }
+    static TagType getChoiceBit(TagType fp) { return (fp >> choiceBitPos) & 1; }
+    static TagType setChoiceBit(TagType fp, TagType choice) {
+        return TagType((fp & pureFpMask) | TagType(choice << choiceBitPos));
+    }
+    /* The alternate bucket and the tag as stored there (choice bit flipped). */
+    static std::tuple<std::size_t, TagType> getAlternateBucketWithNewFp(std::size_t bucket, TagType fp,
+                                                                        std::size_t numBuckets) {
+        const std::size_t alt =
+            cuckoo_b200::AltPolicyBase<KeyType, TagType, bitsPerTag, bucketSize,
+                                       CF_ALT_OFFSET>::getAlternateBucket(bucket, fp, numBuckets);
+        return {alt, TagType(fp ^ choiceBitMask)};
     }
 };
 
@@ -195,7 +253,7 @@ class CuckooFilter {
         c.eviction_policy = Config::evictionPolicy == EvictionPolicy::BFS ? CF_EVICT_BFS : CF_EVICT_DFS;
         c.max_evictions = static_cast<std::uint32_t>(maxEvictions);
         c.block_size = static_cast<std::uint32_t>(blockSize);
-        c.alt_policy = CF_ALT_XOR;
+        c.alt_policy = Config::AltBucketPolicy::alt_policy;
         return c;
     }
 
@@ -311,6 +369,14 @@ class CuckooFilter {
     }
     static std::size_t getAlternateBucket(std::size_t bucket, TagType fp, std::size_t numBuckets) {
         return Config::AltBucketPolicy::getAlternateBucket(bucket, fp, numBuckets);
+    }
+    /* The alternate bucket and the tag as stored there (CuckooFilter.cuh:394-401). */
+    static std::tuple<std::size_t, TagType> getAlternateBucketWithNewFp(std::size_t bucket, TagType fp,
+                                                                        std::size_t numBuckets) {
+        if constexpr (Config::AltBucketPolicy::usesChoiceBit)
+            return Config::AltBucketPolicy::getAlternateBucketWithNewFp(bucket, fp, numBuckets);
+        else
+            return {Config::AltBucketPolicy::getAlternateBucket(bucket, fp, numBuckets), fp};
     }
     static std::size_t calculateNumBuckets(std::size_t capacity) {
         return Config::AltBucketPolicy::calculateNumBuckets(capacity);

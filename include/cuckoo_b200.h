@@ -41,9 +41,15 @@ typedef enum cf_status {
 /* Eviction policy (reference enum class EvictionPolicy, CuckooFilter.cuh:19-22). */
 typedef enum cf_eviction { CF_EVICT_BFS = 0, CF_EVICT_DFS = 1 } cf_eviction;
 
-/* Alternate-bucket policy (reference bucket_policies.cuh).  Only the XOR policy
- * (XorAltBucketPolicy, :15-84) is implemented. */
-typedef enum cf_alt_policy { CF_ALT_XOR = 0 } cf_alt_policy;
+/* Alternate-bucket policy (reference bucket_policies.cuh): XorAltBucketPolicy
+ * (:15-84; power-of-two bucket count), AddSubAltBucketPolicy (:95-177; even
+ * bucket count, primary buckets in the first half, alternates in the second)
+ * and OffsetAltBucketPolicy (:179-350; any bucket count, the tag's top bit is
+ * a choice bit: 0 in the primary bucket, 1 in the alternate).  AddSub and
+ * Offset are built for 16-bit tags in 16-slot buckets (the reference's
+ * bucket_policy_benchmark.cu:16-17 geometry); their batches always take the
+ * random-probe path. */
+typedef enum cf_alt_policy { CF_ALT_XOR = 0, CF_ALT_ADDSUB = 1, CF_ALT_OFFSET = 2 } cf_alt_policy;
 
 /*
  * Runtime form of CuckooConfig<T, bitsPerTag, maxEvictions, blockSize,
@@ -105,6 +111,11 @@ int cf_config_supported(const cf_config* cfg);
  * nextPowerOfTwo(ceil(capacity / bucket_size)) (XorAltBucketPolicy::calculateNumBuckets,
  * bucket_policies.cuh:80-83). */
 uint64_t cf_num_buckets_for(uint64_t capacity, uint32_t bucket_size);
+
+/* calculateNumBuckets of an alternate-bucket policy (cf_alt_policy): XOR as
+ * cf_num_buckets_for; AddSub ceil(capacity / bucket_size) rounded up to even
+ * (bucket_policies.cuh:166-176); Offset ceil(capacity / bucket_size) (:346-349). */
+uint64_t cf_num_buckets_for_policy(uint64_t capacity, uint32_t bucket_size, uint32_t alt_policy);
 
 /* explicit CuckooFilter(size_t capacity) (CuckooFilter.cuh:420-428): allocates
  * and zeroes the table on the current device. */
@@ -240,8 +251,9 @@ int cf_get_option(cf_filter* f, int option, uint64_t* value);
 int cf_store_table(cf_filter* f, void* dst, uint64_t bytes, void* stream);
 
 /* static getCandidateBuckets(key, numBuckets) (CuckooFilter.cuh:366-369 ->
- * XorAltBucketPolicy::getCandidateBuckets, bucket_policies.cuh:46-61) for n
- * HOST keys: the kernels' hashing evaluated on the CPU.  Any of i1/i2/fp may be NULL. */
+ * the policy's getCandidateBuckets, bucket_policies.cuh:46-61, :125-140,
+ * :232-256) for n HOST keys: the kernels' hashing evaluated on the CPU.  fp is
+ * the tag as stored in the primary bucket i1.  Any of i1/i2/fp may be NULL. */
 int cf_hash_candidates(const cf_config* cfg, uint64_t num_buckets, const void* h_keys, uint64_t n, uint64_t* i1,
                        uint64_t* i2, uint32_t* fp);
 
@@ -250,8 +262,11 @@ int cf_hash_candidates(const cf_config* cfg, uint64_t num_buckets, const void* h
 int cf_hash64(uint32_t value_bytes, const void* h_values, uint64_t n, uint64_t* out);
 
 /* static getAlternateBucket(bucket, fp, numBuckets) (CuckooFilter.cuh:378-381 ->
- * XorAltBucketPolicy::getAlternateBucket, bucket_policies.cuh:72-74) for n HOST
- * (bucket, tag) pairs: out[i] = buckets[i] ^ (xxHash64(tag as TagType) & (num_buckets - 1)). */
+ * the policy's getAlternateBucket, bucket_policies.cuh:72-74, :150-160, :300-323)
+ * for n HOST (bucket, tag) pairs of cfg's alternate-bucket policy.  XOR:
+ * out[i] = buckets[i] ^ (xxHash64(tag as TagType) & (num_buckets - 1)).  Under
+ * the Offset policy the tag is stored in the alternate bucket with its choice
+ * bit (1 << (bits_per_tag - 1)) flipped. */
 int cf_alt_buckets(const cf_config* cfg, uint64_t num_buckets, const uint64_t* buckets, const uint32_t* tags,
                    uint64_t n, uint64_t* out);
 

@@ -327,6 +327,13 @@ REF_GPU_CONFIGS = {
     (8, 8, 16, POLICY_BFS, 500, 4): 12,
     (8, 16, 16, POLICY_DFS, 500, 4): 13,
     (8, 16, 16, POLICY_BFS, 16, 4): 14,
+    # other alternate-bucket policies: (..., word_bytes, alt_policy)
+    (8, 16, 16, POLICY_BFS, 500, 8, ALT_ADDSUB): 15,
+    (8, 16, 16, POLICY_DFS, 500, 8, ALT_ADDSUB): 16,
+    (8, 16, 16, POLICY_BFS, 500, 8, ALT_OFFSET): 17,
+    (8, 16, 16, POLICY_DFS, 500, 8, ALT_OFFSET): 18,
+    (8, 16, 16, POLICY_DFS, 16, 8, ALT_OFFSET): 19,
+    (8, 16, 16, POLICY_DFS, 16, 8, ALT_ADDSUB): 20,
 }
 
 _ref_gpu = None
@@ -362,9 +369,14 @@ def ref_gpu():
 class RefGpuFilter:
     """The reference's CuckooFilter<Config> (managed-memory object) on cuda:0."""
 
-    def __init__(self, key_bytes, bits, bucket_size, policy, max_evictions, capacity, word_bytes=8):
+    def __init__(self, key_bytes, bits, bucket_size, policy, max_evictions, capacity, word_bytes=8,
+                 alt_policy=ALT_XOR):
         key = (key_bytes, bits, bucket_size, policy, max_evictions)
-        self.cfg = REF_GPU_CONFIGS[key if word_bytes == 8 else key + (word_bytes,)]
+        if alt_policy != ALT_XOR:
+            key = key + (word_bytes, alt_policy)
+        elif word_bytes != 8:
+            key = key + (word_bytes,)
+        self.cfg = REF_GPU_CONFIGS[key]
         self.L = ref_gpu()
         self.h = self.L.refg_create(self.cfg, capacity)
         if not self.h:

@@ -36,6 +36,13 @@ using XorU64_8_BFS_W32 = CuckooConfig<uint64_t, 8, 500, 256, 16, XorAltBucketPol
 using XorU64_16_DFS_W32 = CuckooConfig<uint64_t, 16, 500, 256, 16, XorAltBucketPolicy, EvictionPolicy::DFS, uint32_t>;
 using XorU64_16_BFS_E16_W32 =
     CuckooConfig<uint64_t, 16, 16, 256, 16, XorAltBucketPolicy, EvictionPolicy::BFS, uint32_t>;
+// AddSub and Offset alternate-bucket policies (benchmark/bucket_policy_benchmark.cu:16-17)
+using AddSubU64_16_BFS = CuckooConfig<uint64_t, 16, 500, 256, 16, AddSubAltBucketPolicy, EvictionPolicy::BFS>;
+using AddSubU64_16_DFS = CuckooConfig<uint64_t, 16, 500, 256, 16, AddSubAltBucketPolicy, EvictionPolicy::DFS>;
+using OffsetU64_16_BFS = CuckooConfig<uint64_t, 16, 500, 256, 16, OffsetAltBucketPolicy, EvictionPolicy::BFS>;
+using OffsetU64_16_DFS = CuckooConfig<uint64_t, 16, 500, 256, 16, OffsetAltBucketPolicy, EvictionPolicy::DFS>;
+using OffsetU64_16_DFS_E16 = CuckooConfig<uint64_t, 16, 16, 256, 16, OffsetAltBucketPolicy, EvictionPolicy::DFS>;
+using AddSubU64_16_DFS_E16 = CuckooConfig<uint64_t, 16, 16, 256, 16, AddSubAltBucketPolicy, EvictionPolicy::DFS>;
 
 template <typename Cfg>
 struct Shim {
@@ -97,6 +104,8 @@ const Ops kOps[] = {
     ops_of<XorU32_16_DFS>(),     ops_of<XorU64_16_DFS_E16>(), ops_of<XorU64_16_BFS_E16>(),
     ops_of<XorU64_32_DFS_E16>(), ops_of<XorU64_32_BFS_E16>(), ops_of<XorU64_8_DFS_W32>(),
     ops_of<XorU64_8_BFS_W32>(),  ops_of<XorU64_16_DFS_W32>(), ops_of<XorU64_16_BFS_E16_W32>(),
+    ops_of<AddSubU64_16_BFS>(),  ops_of<AddSubU64_16_DFS>(),  ops_of<OffsetU64_16_BFS>(),
+    ops_of<OffsetU64_16_DFS>(),  ops_of<OffsetU64_16_DFS_E16>(), ops_of<AddSubU64_16_DFS_E16>(),
 };
 constexpr int kNumOps = sizeof(kOps) / sizeof(kOps[0]);
 

@@ -235,6 +235,35 @@ void SortedInsertAndHelpers(std::mt19937& rng) {
     EXPECT(threw, "a NULL batch raises cuckoo_b200::Error(CF_ERR_INVALID)");
 }
 
+// The AddSub and Offset alternate-bucket policies through the drop-in
+// (the reference's bucket_policy_benchmark.cu:16-17 configurations).
+template <template <typename, typename, std::size_t, std::size_t> class Policy>
+void PolicyFilter(std::mt19937& rng) {
+    using Cfg = CuckooConfig<uint64_t, 16, 500, 128, 16, Policy>;
+    using F = CuckooFilter<Cfg>;
+    const size_t cap = 100003;  // not a power of two: these policies keep ceil(cap / 16) buckets
+    F f(cap);
+    EXPECT(f.getNumBuckets() == F::calculateNumBuckets(cap) && f.getNumBuckets() >= cap / 16, "bucket count");
+    std::vector<uint64_t> keys(static_cast<size_t>(0.9 * f.capacity()));
+    std::uniform_int_distribution<uint64_t> dist;
+    for (auto& k : keys) k = dist(rng);
+    thrust::device_vector<uint64_t> d(keys.begin(), keys.end());
+    EXPECT(f.insertMany(d) == keys.size(), "all keys stored at 90% load");
+    thrust::device_vector<uint8_t> out(keys.size());
+    f.containsMany(d, out);
+    EXPECT(count_true(host(out)) == keys.size(), "no false negatives");
+    auto [i1, i2, fp] = F::getCandidateBuckets(keys[0], f.getNumBuckets());
+    auto [alt, afp] = F::getAlternateBucketWithNewFp(i1, fp, f.getNumBuckets());
+    EXPECT(alt == i2, "alternate of the primary bucket is i2");
+    auto [back, bfp] = F::getAlternateBucketWithNewFp(alt, afp, f.getNumBuckets());
+    EXPECT(back == i1 && bfp == fp, "moving twice returns the tag home");
+    thrust::device_vector<uint8_t> del(keys.size());
+    EXPECT(f.deleteMany(d, del) == 0, "every key deleted");
+}
+
+void AddSubPolicy(std::mt19937& rng) { PolicyFilter<AddSubAltBucketPolicy>(rng); }
+void OffsetPolicy(std::mt19937& rng) { PolicyFilter<OffsetAltBucketPolicy>(rng); }
+
 }  // namespace
 
 int main() {
@@ -253,7 +282,9 @@ int main() {
                  {"DeleteAndReinsert", DeleteAndReinsert},
                  {"LoadFactorAfterDeletion", LoadFactorAfterDeletion},
                  {"DeleteDuplicates", DeleteDuplicates},
-                 {"SortedInsertAndHelpers", SortedInsertAndHelpers}};
+                 {"SortedInsertAndHelpers", SortedInsertAndHelpers},
+                 {"AddSubPolicy", AddSubPolicy},
+                 {"OffsetPolicy", OffsetPolicy}};
     for (const Case& c : cases) {
         std::mt19937 rng(42);  // the reference's fixture seeds every case with 42
         const int before = g_failures;

@@ -152,5 +152,7 @@ def test_python_config_mirror(cfb):
     c = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16)
     assert (c.maxEvictions, c.blockSize, c.bucketSize, c.evictionPolicy) == (500, 256, 16, cfb.EvictionPolicy.DFS)
     assert c.TagType == "uint16_t" and c.key_bytes == 8
+    assert cfb.CuckooConfig(T="uint64", bitsPerTag=16, AltBucketPolicy="AddSubAltBucketPolicy").to_c().alt_policy == 1
+    assert cfb.CuckooConfig(T="uint64", bitsPerTag=16, AltBucketPolicy="OffsetAltBucketPolicy").to_c().alt_policy == 2
     with pytest.raises(cfb.CuckooError):
-        cfb.CuckooConfig(T="uint64", bitsPerTag=16, AltBucketPolicy="AddSubAltBucketPolicy").to_c()
+        cfb.CuckooConfig(T="uint64", bitsPerTag=16, AltBucketPolicy="ModuloAltBucketPolicy").to_c()

@@ -90,4 +90,4 @@ def test_reference_suite_through_cpp_header(cfb):
     exe = build_test_program()
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "0 failures" in r.stdout and r.stdout.count("[  OK  ]") == 13, r.stdout
+    assert "0 failures" in r.stdout and r.stdout.count("[  OK  ]") == 15, r.stdout

@@ -1,0 +1,167 @@
+"""AddSub and Offset alternate-bucket policies on the GPU (reference
+include/bucket_policies.cuh:95-350, used by the filter at
+CuckooFilter.cuh:1033-1059, :1091-1094, :1109-1112 and in its evictions).
+
+Exact checks against the oracle: one-key-per-call insert images (evictions,
+failed chains and their undo included), lookups on identical images, one-key
+deletes.  The oracle's policy code is pinned to the reference's own kernels
+built with these policies.  Bulk batches are checked through invariants (the
+Offset policy's choice bit is set exactly on tags in their alternate bucket).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+from test_gpu_parity import dev, host_u8, image  # noqa: E402
+
+NAMES = {1: "AddSubAltBucketPolicy", 2: "OffsetAltBucketPolicy"}
+
+
+def make(cfb, orc, alt, kb=8, policy=1, max_ev=500, cap=1 << 12):
+    cfg = cfb.CuckooConfig(T="uint64" if kb == 8 else "uint32", bitsPerTag=16, bucketSize=16, maxEvictions=max_ev,
+                           evictionPolicy=cfb.EvictionPolicy(policy), AltBucketPolicy=NAMES[alt])
+    f = cfb.CuckooFilter(cfg, cap)
+    o = orc.OracleFilter(key_bytes=kb, bits=16, bucket_size=16, policy=policy, max_evictions=max_ev, capacity=cap,
+                         mode=orc.MODE_CONSERVING, alt_policy=alt)
+    assert f.getNumBuckets() == o.nb == cfb.CuckooFilter.calculateNumBuckets(cap, 16, NAMES[alt])
+    return f, o
+
+
+SEQ = [
+    # alt, key_bytes, eviction policy, max_ev, capacity (not a power of two: 16 * 250 + 16 * 3), fill
+    (1, 8, 0, 500, 4048, 0.97),
+    (1, 8, 1, 500, 4048, 0.97),
+    (2, 8, 0, 500, 4048, 0.97),
+    (2, 8, 1, 500, 4048, 0.97),
+    (2, 4, 0, 500, 4048, 0.97),
+    (1, 4, 1, 500, 4048, 0.97),
+    (2, 8, 1, 16, 4048, 1.00),
+    (1, 8, 1, 16, 4048, 1.00),
+    (2, 8, 0, 16, 4000, 1.00),
+]
+
+
+@pytest.mark.parametrize("alt,kb,policy,max_ev,cap,fill", SEQ)
+def test_sequential_image_bit_exact(cfb, orc, alt, kb, policy, max_ev, cap, fill):
+    f, o = make(cfb, orc, alt, kb, policy, max_ev, cap)
+    keys = orc.splitmix64(500 + alt * 10 + policy, int(fill * f.capacity()))
+    if kb == 4:
+        keys = keys.astype(np.uint32)
+    d = dev(keys)
+    out = torch.empty(1, dtype=torch.bool, device="cuda")
+    got = np.empty(len(keys), np.uint8)
+    for i in range(len(keys)):
+        f.insertMany(d[i:i + 1], d_output=out)
+        got[i] = int(out.item())
+    n_ok, want = o.insert(keys, out=True)
+    assert np.array_equal(got, want), f"first differing key {int(np.argmax(got != want))}"
+    assert np.array_equal(image(f), o.table)
+    st = f.stats()
+    assert st["occupied"] == n_ok == f.countOccupiedSlots() and st["lost"] == 0
+    if fill >= 1.0:
+        assert st["failed"] > 0, "case meant to exercise failed chains"
+
+
+@pytest.mark.parametrize("cfg_key,cap", [((2, 0, 500), 4048), ((2, 1, 500), 4048), ((1, 0, 500), 4048),
+                                         ((1, 1, 500), 4048), ((2, 1, 16), 4048), ((1, 1, 16), 4048)])
+def test_reference_kernels_with_policy_match_oracle(cfb, orc, cfg_key, cap):
+    """The reference's own kernels with the policy, one key per launch, against
+    the oracle's reference mode up to the first failed chain."""
+    if orc.ref_gpu() is None:
+        pytest.skip("oracle/_ref/libref_gpu.so not built")
+    alt, policy, max_ev = cfg_key
+    ref = orc.RefGpuFilter(8, 16, 16, policy, max_ev, cap, alt_policy=alt)
+    scratch = None
+    try:
+        o = orc.OracleFilter(key_bytes=8, bits=16, bucket_size=16, policy=policy, max_evictions=max_ev,
+                             capacity=cap, mode=orc.MODE_REFERENCE, alt_policy=alt)
+        assert ref.num_buckets() == o.nb
+        cfg = cfb.CuckooConfig(T="uint64", bitsPerTag=16, bucketSize=16, AltBucketPolicy=NAMES[alt])
+        scratch = cfb.CuckooFilter(cfg, cap)
+        ptr, nbytes = ref.table()
+        keys = orc.splitmix64(800 + alt * 10 + policy, int(0.98 * o.nb * 16))
+        d = dev(keys)
+        prev = 0
+        for i in range(len(keys)):
+            occ = ref.insert(d[i:i + 1].data_ptr(), 1)
+            ok = occ - prev
+            prev = occ
+            want = o.insert(keys[i:i + 1])
+            assert ok == want, i
+            if want == 0 or i == len(keys) - 1 or i % 500 == 0:
+                scratch.load_table(ptr, nbytes)
+                assert np.array_equal(image(scratch), o.table), f"image differs after key {i}"
+            if want == 0:
+                break
+    finally:
+        ref.close()
+        if scratch is not None:
+            scratch.close()
+
+
+@pytest.mark.parametrize("alt", [1, 2])
+def test_contains_and_delete_on_identical_image(cfb, orc, alt):
+    f, o = make(cfb, orc, alt, cap=50_000)
+    keys = orc.splitmix64(61 + alt, int(0.95 * f.capacity()))
+    o.insert(keys)
+    f.load_table(torch.from_numpy(o.table).cuda())
+    neg = orc.splitmix64(62 + alt, 100_000)
+    q = np.concatenate([keys, neg])
+    assert np.array_equal(host_u8(f.containsMany(dev(q))), o.contains(q))
+    dels = np.concatenate([keys[::3], orc.splitmix64(63, 200), keys[:50]])
+    d = dev(dels)
+    out = torch.empty(1, dtype=torch.bool, device="cuda")
+    got = np.empty(len(dels), np.uint8)
+    for i in range(len(dels)):
+        f.deleteMany(d[i:i + 1], out)
+        got[i] = int(out.item())
+    _, want = o.delete(dels)
+    assert np.array_equal(got, want)
+    assert np.array_equal(image(f), o.table)
+
+
+@pytest.mark.parametrize("sorted_", [False, True])
+@pytest.mark.parametrize("alt,policy", [(1, 0), (1, 1), (2, 0), (2, 1)])
+def test_bulk_invariants(cfb, orc, alt, policy, sorted_):
+    f, o = make(cfb, orc, alt, policy=policy, cap=1_000_000)
+    keys = orc.splitmix64(1, int(0.95 * f.capacity()))
+    d = dev(keys)
+    ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
+    occ = f.insertManySorted(d, d_output=ok_t) if sorted_ else f.insertMany(d, d_output=ok_t)
+    ok = host_u8(ok_t).astype(bool)
+    st = f.stats()
+    assert occ == ok.sum() == st["occupied"] == f.countOccupiedSlots() and st["lost"] == 0
+    assert st["failed"] == len(keys) - ok.sum() and st["failed"] <= len(keys) // 1000
+    assert host_u8(f.containsMany(d[torch.from_numpy(ok).cuda()])).all(), "false negative"
+    slots = image(f).view(np.uint16).reshape(o.nb, 16)
+    stored = keys[ok]
+    i1, i2, fp = o.candidates(stored)
+    errs = orc.check_invariants(slots, o.alt_map(), i1, i2, fp, norm=o.pure_tag)
+    assert not errs, errs
+    if alt == 2:
+        # a tag carries the choice bit exactly when it sits in its alternate
+        # bucket: (primary bucket, tag without the bit) of the table entries
+        # equals (i1, fp) of the stored keys, as multisets
+        b, s = np.nonzero(slots)
+        b = b.astype(np.uint64)
+        t = slots[b.astype(np.int64), s].astype(np.uint64)
+        prim = np.where(t & np.uint64(0x8000), o.alt_map()(b, t), b)
+        got = np.stack([prim, t & np.uint64(0x7FFF)], 1)
+        want = np.stack([i1.astype(np.uint64), fp.astype(np.uint64)], 1)
+        assert np.array_equal(got[np.lexsort(got.T[::-1])], want[np.lexsort(want.T[::-1])])
+    half = len(stored) // 2
+    out = torch.empty(half, dtype=torch.bool, device="cuda")
+    occ1 = f.deleteMany(dev(stored[:half]), out)
+    assert host_u8(out).all() and occ1 == occ - half
+    assert host_u8(f.containsMany(dev(stored[half:]))).all()
+    f.close()
+
+
+def test_policies_reject_filter_sets(cfb, orc):
+    cfg = cfb.CuckooConfig(T="uint64", bitsPerTag=16, bucketSize=16, AltBucketPolicy="OffsetAltBucketPolicy")
+    with pytest.raises(cfb.CuckooError):
+        cfb.CuckooFilterSet(cfg, [1 << 12, 1 << 12])
