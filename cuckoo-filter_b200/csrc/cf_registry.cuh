@@ -158,6 +158,11 @@ constexpr uintptr_t key_vec_align() {
 template <class C>
 struct Launchers {
     using Key = typename C::Key;
+    // keys per thread; buckets wider than 64 bytes keep fewer in flight so
+    // their images stay in registers
+    static constexpr int CKPT = C::bucket_bytes > 64 ? 2 : kContainsKPT;
+    static constexpr int DKPT = C::bucket_bytes > 64 ? 1 : kDeleteKPT;
+    static constexpr int IKPT = C::bucket_bytes > 64 ? 1 : kInsertKPT;
 
     template <int K>
     static cudaError_t contains_k(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
@@ -171,12 +176,12 @@ struct Launchers {
         switch (L.kpt) {
             case 1: return contains_k<1>(t, keys, n, out, L);
             case 2: return contains_k<2>(t, keys, n, out, L);
-            default: return contains_k<kContainsKPT>(t, keys, n, out, L);
+            default: return contains_k<CKPT>(t, keys, n, out, L);
         }
     }
     static cudaError_t remove(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
         if (n == 0) return cudaSuccess;
-        constexpr int K = kDeleteKPT;
+        constexpr int K = DKPT;
         const int grid = L.full_grid ? full_grid_for(n, L.block, K) : grid_for(n, L.block, K, L.max_grid);
         { k_delete<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
                                                        aligned(keys, key_vec_align<C, K>()), aligned(out, K)); CF_COUNT_LAUNCH(); }
@@ -185,7 +190,7 @@ struct Launchers {
     static cudaError_t insert(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L,
                               uint32_t policy_bfs, uint32_t max_ev) {
         if (n == 0) return cudaSuccess;
-        constexpr int K = kInsertKPT;
+        constexpr int K = IKPT;
         const int grid = L.full_grid ? full_grid_for(n, L.block, K) : grid_for(n, L.block, K, L.max_grid);
         { k_insert<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
                                                        aligned(keys, key_vec_align<C, K>()), aligned(out, K),
@@ -207,11 +212,11 @@ struct Launchers {
     static cudaError_t occupancy(int kid, int block, int* bps) {
         switch (kid) {
             case KID_CONTAINS:
-                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_contains<C, kContainsKPT>, block, 0);
+                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_contains<C, CKPT>, block, 0);
             case KID_DELETE:
-                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_delete<C, kDeleteKPT>, block, 0);
+                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_delete<C, DKPT>, block, 0);
             default:
-                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_insert<C, kInsertKPT>, block, 0);
+                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_insert<C, IKPT>, block, 0);
         }
     }
 
@@ -479,9 +484,9 @@ struct Launchers {
         o.word_bytes = C::word_bytes;
         o.alt_policy = C::alt_policy;
         o.bucket_bytes = C::bucket_bytes;
-        o.kpt[KID_CONTAINS] = kContainsKPT;
-        o.kpt[KID_DELETE] = kDeleteKPT;
-        o.kpt[KID_INSERT] = kInsertKPT;
+        o.kpt[KID_CONTAINS] = CKPT;
+        o.kpt[KID_DELETE] = DKPT;
+        o.kpt[KID_INSERT] = IKPT;
         o.contains = contains;
         o.remove = remove;
         o.insert = insert;

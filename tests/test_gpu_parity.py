@@ -76,6 +76,8 @@ SEQ_CASES = [
     (4, 16, 16, 1, 500, 1 << 12, 0.97),
     (8, 16, 4, 0, 32, 1 << 10, 1.00),
     (8, 8, 64, 1, 64, 1 << 12, 0.99),
+    (8, 16, 64, 1, 500, 1 << 12, 0.97),  # 128-byte buckets
+    (8, 16, 64, 0, 16, 1 << 12, 1.00),
 ]
 
 
@@ -147,7 +149,8 @@ def _ref_image(cfb, ref, kb, bits, bs) -> np.ndarray:
         scratch.close()
 
 
-LOOKUP_CASES = [(8, 16, 16), (8, 8, 16), (8, 32, 8), (4, 16, 16), (8, 16, 4), (8, 8, 64), (8, 16, 32), (4, 32, 16)]
+LOOKUP_CASES = [(8, 16, 16), (8, 8, 16), (8, 32, 8), (4, 16, 16), (8, 16, 4), (8, 8, 64), (8, 16, 32), (4, 32, 16),
+                (8, 16, 64)]
 
 
 @pytest.mark.parametrize("kb,bits,bs", LOOKUP_CASES)
@@ -202,7 +205,8 @@ def _stored_invariants(f, o, orc, stored_keys):
     return orc.check_invariants(slots, alt_fn(orc, o), i1, i2, fp)
 
 
-BULK_CASES = [(8, 16, 16, 0), (8, 16, 16, 1), (8, 8, 16, 0), (8, 32, 8, 1), (8, 32, 8, 0), (4, 16, 16, 1)]
+BULK_CASES = [(8, 16, 16, 0), (8, 16, 16, 1), (8, 8, 16, 0), (8, 32, 8, 1), (8, 32, 8, 0), (4, 16, 16, 1),
+              (8, 16, 64, 0)]
 
 
 @pytest.mark.parametrize("staging", ["random", "region"])
