@@ -1005,11 +1005,38 @@ def run_grid(args) -> dict:
 # ------------------------------------------------------- alternate-bucket policies
 
 
+def _time_fill_query_delete(f, path, fill, query, dele, q_out, stream) -> dict:
+    """One cleared fill (insertMany or insertManySorted), lookups and deletes,
+    each timed with CUDA events on `stream`."""
+    import torch
+
+    f.clear(stream)
+    f.resetEvictionCount()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record(stream)
+    if path == "insertMany":
+        f.insertManyAsync(fill, stream=stream)
+    else:
+        f.insertManySorted(fill, stream=stream)
+    e[1].record(stream)
+    f.containsManyAsync(query, q_out, stream=stream)
+    e[2].record(stream)
+    f.deleteManyAsync(dele, stream=stream)
+    e[3].record(stream)
+    torch.cuda.synchronize()
+    st = f.stats()
+    return {"insert_gkeys_s": fill.numel() / e[0].elapsed_time(e[1]) / 1e6,
+            "lookup_gkeys_s": query.numel() / e[1].elapsed_time(e[2]) / 1e6,
+            "delete_gkeys_s": dele.numel() / e[2].elapsed_time(e[3]) / 1e6,
+            "failed": st["failed"], "lost": st["lost"], "evictions": st["evictions"],
+            "lookup_hits": int(q_out.sum().item())}
+
+
 def run_policies(args) -> dict:
     """The three alternate-bucket policies on the large workload's keys
     (the reference's bucket_policy_benchmark.cu configurations: 16-bit tags,
-    16-slot buckets, DFS): 2^31 slots filled to 0.95 with insertMany, 2^28
-    lookups (50 % positive), 2^26 deletes."""
+    16-slot buckets, DFS): 2^31 slots filled to 0.95 with insertMany and with
+    insertManySorted, 2^28 lookups (50 % positive), 2^26 deletes."""
     import torch
 
     from __graft_entry__ import package
@@ -1026,33 +1053,20 @@ def run_policies(args) -> dict:
         cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16, bucketSize=16, maxEvictions=500,
                                evictionPolicy=cfb.EvictionPolicy.DFS, AltBucketPolicy=name)
         f = cfb.CuckooFilter(cfg, base["capacity"])
-        res = {}
-        for _ in range(2):  # the first pass warms the caches
-            f.clear(stream)
-            f.resetEvictionCount()
-            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-            e[0].record(stream)
-            f.insertManyAsync(fill, stream=stream)
-            e[1].record(stream)
-            f.containsManyAsync(query, q_out, stream=stream)
-            e[2].record(stream)
-            f.deleteManyAsync(dele, stream=stream)
-            e[3].record(stream)
-            torch.cuda.synchronize()
-            st = f.stats()
-            res = {"policy": name, "num_buckets": f.getNumBuckets(), "table_bytes": f.sizeInBytes(),
-                   "insert_gkeys_s": fill.numel() / e[0].elapsed_time(e[1]) / 1e6,
-                   "lookup_gkeys_s": query.numel() / e[1].elapsed_time(e[2]) / 1e6,
-                   "delete_gkeys_s": dele.numel() / e[2].elapsed_time(e[3]) / 1e6,
-                   "failed": st["failed"], "lost": st["lost"], "evictions": st["evictions"],
-                   "lookup_hits": int(q_out.sum().item())}
-        rows.append(res)
-        print(json.dumps(res), file=sys.stderr, flush=True)
+        f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
+        for path in ("insertMany", "insertManySorted"):
+            res = {}
+            for _ in range(2):  # the first pass warms the workspace and the caches
+                res = _time_fill_query_delete(f, path, fill, query, dele, q_out, stream)
+            res = {"policy": name, "insert_path": path, "num_buckets": f.getNumBuckets(),
+                   "table_bytes": f.sizeInBytes(), **res}
+            rows.append(res)
+            print(json.dumps(res), file=sys.stderr, flush=True)
         f.close()
     return {"form": "policies", "metric": "Gkeys/s per op for each alternate-bucket policy", "unit": "Gkeys/s",
             "n_gpus": 1, "dtype": "u64", "data": "synthetic: splitmix64 keys (large workload)",
-            "config": {"workload": "2^31 slots, 16/16, DFS, insertMany to 0.95 (2 040 109 465 keys), 2^28 lookups "
-                                   "50% positive, 2^26 deletes"}, "rows": rows}
+            "config": {"workload": "2^31 slots, 16/16, DFS, insertMany / insertManySorted to 0.95 (2 040 109 465 "
+                                   "keys), 2^28 lookups 50% positive, 2^26 deletes"}, "rows": rows}
 
 
 # ------------------------------------------------------------ reference arm

@@ -34,7 +34,8 @@ struct cf_filter {
     int max_grid_aux;
     int sms;
     // segment-staged path
-    bool seg_ok;            // the staged paths apply: XOR policy, packed (bucket, tag) entries fit in 64 bits
+    bool seg_ok;            // the segment-staged path applies: packed (bucket, tag) entries fit in 64 bits
+    bool rg_ok;             // the region-staged path applies (XOR policy)
     SegGeom geom;
     void* ws;               // workspace (grown on demand, freed with the filter)
     uint64_t ws_bytes;
@@ -194,19 +195,24 @@ int finish(cf_filter* f, void* stream, uint64_t* occupied_out) {
 
 int ilog2(uint64_t v) { return 63 - __builtin_clzll(v); }
 
+// ceil(log2(v)) for v >= 1
+int clog2(uint64_t v) { return v <= 1 ? 0 : ilog2(v - 1) + 1; }
+
 void init_geometry(cf_filter* f) {
     const uint64_t bb = f->ops->bucket_bytes;
     uint64_t sb = kSegBytes / bb;
     if (sb > f->num_buckets) sb = f->num_buckets;
-    f->geom.sb_log2 = ilog2(sb);
-    f->geom.nseg = f->num_buckets / sb;
+    f->geom.sb_log2 = ilog2(sb);  // a power of two at most the bucket count
+    sb = 1ull << f->geom.sb_log2;
+    // the last segment is partial when the bucket count (AddSub and Offset
+    // policies) is not a multiple of the segment
+    f->geom.nseg = (f->num_buckets + sb - 1) / sb;
     f->geom.seg_shift = static_cast<int>(f->cfg.bits_per_tag) + f->geom.sb_log2;
-    const int seg_bits = f->geom.nseg > 1 ? ilog2(f->geom.nseg) : 0;
+    const int seg_bits = clog2(f->geom.nseg);
     f->geom.passes = seg_bits == 0 ? 1 : (seg_bits + kRadixBits - 1) / kRadixBits;
-    // (bucket << bits) | tag must fit in 64 bits for every bucket index, and
-    // the staged paths exist for the XOR policy only
-    f->seg_ok = ilog2(f->num_buckets) + static_cast<int>(f->cfg.bits_per_tag) <= 64 && f->ops->seg_chunk &&
-                f->ops->rg_chunk;
+    // (bucket << bits) | tag must fit in 64 bits for every bucket index
+    f->seg_ok = clog2(f->num_buckets) + static_cast<int>(f->cfg.bits_per_tag) <= 64 && f->ops->seg_chunk;
+    f->rg_ok = f->seg_ok && f->ops->rg_chunk;
     // regions of ~kRgRegionBytes (or CF_OPT_REGION_BYTES), at most kRgMaxRegions of them
     const int nb_log2 = ilog2(f->num_buckets);
     const uint64_t rbytes = f->rg_bytes ? f->rg_bytes : kRgRegionBytes;
@@ -362,10 +368,10 @@ Path choose_path(const cf_filter* f, int op, uint64_t n, bool sorted_insert) {
     switch (f->staging) {
         case CF_STAGING_RANDOM: return sorted_insert ? PATH_SEGMENT : PATH_RANDOM;
         case CF_STAGING_SEGMENT: return PATH_SEGMENT;
-        case CF_STAGING_REGION: return PATH_REGION;
+        case CF_STAGING_REGION: return f->rg_ok ? PATH_REGION : PATH_SEGMENT;
         default: break;
     }
-    if (n >= region_threshold(f, op)) return PATH_REGION;
+    if (f->rg_ok && n >= region_threshold(f, op)) return PATH_REGION;
     if (sorted_insert) return PATH_SEGMENT;
     if (op != SEG_INSERT && n >= segmented_threshold(f, op)) return PATH_SEGMENT;
     return PATH_RANDOM;
@@ -913,8 +919,7 @@ int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8
         return fail(CF_ERR_INVALID, "%llu keys exceed the %llu-key limit of cf_insert_sorted_noalloc; split the batch",
                     static_cast<unsigned long long>(n), static_cast<unsigned long long>(kNoAllocMaxKeys));
     if (!f->seg_ok)
-        return fail(CF_ERR_UNSUPPORTED, "the segment-staged path does not apply to this table (alternate-bucket "
-                                        "policy other than XOR, or bucket index and tag wider than 64 bits)");
+        return fail(CF_ERR_UNSUPPORTED, "bucket index and tag do not fit one 64-bit entry for this table");
     if (f->geom.nseg > kNoAllocMaxSegments)
         return fail(CF_ERR_UNSUPPORTED, "table of %llu segments exceeds the %llu-segment limit of the fixed scratch",
                     static_cast<unsigned long long>(f->geom.nseg), static_cast<unsigned long long>(kNoAllocMaxSegments));

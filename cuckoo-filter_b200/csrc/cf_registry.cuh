@@ -493,12 +493,9 @@ struct Launchers {
         o.count = count;
         o.probe = probe;
         o.occupancy = occupancy;
-        // the staged paths sort packed (bucket, tag) entries by the XOR
-        // policy's power-of-two bucket index; other policies probe at random
-        if constexpr (C::alt_policy == ALT_XOR) {
-            o.seg_chunk = seg_chunk;
-            o.rg_chunk = rg_chunk;
-        }
+        o.seg_chunk = seg_chunk;
+        // the region-staged path is kept for the XOR policy only
+        if constexpr (C::alt_policy == ALT_XOR) o.rg_chunk = rg_chunk;
         return o;
     }
 };

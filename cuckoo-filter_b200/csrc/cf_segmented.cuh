@@ -494,7 +494,6 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
     __shared__ unsigned long long s_base;
     constexpr int WPB = C::bucket_bytes / 8;  // 64-bit words per bucket
     const uint64_t sb = 1ull << sb_log2;
-    const uint32_t seg_words = static_cast<uint32_t>(sb * WPB);
     const uint32_t tid = threadIdx.x, lane = tid & 31;
     uint32_t n_ok = 0;
     bool err = false;
@@ -502,11 +501,16 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
         const uint32_t lo = start[s], hi = start[s + 1];
         if (lo == hi) continue;
         uint64_t* gseg = reinterpret_cast<uint64_t*>(t.buckets + (s << sb_log2) * C::bucket_bytes);
-        if (seg_words % 2 == 0) {
+        // the last segment of a table whose bucket count is not a multiple of
+        // the segment (AddSub and Offset policies) is partial
+        const uint64_t left = t.nb_mask + 1 - (s << sb_log2);
+        const uint32_t nbk = left < sb ? static_cast<uint32_t>(left) : static_cast<uint32_t>(sb);
+        const uint32_t words = nbk * WPB;
+        if (words % 2 == 0) {
             // 16-byte streaming loads, 8 per thread in flight
             const ulonglong2* g2 = reinterpret_cast<const ulonglong2*>(gseg);
             ulonglong2* s2 = reinterpret_cast<ulonglong2*>(seg);
-            const uint32_t pairs = seg_words / 2;
+            const uint32_t pairs = words / 2;
             for (uint32_t w0 = tid; w0 < pairs; w0 += blockDim.x * 8) {
                 ulonglong2 v[8];
 #pragma unroll
@@ -516,8 +520,8 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
                 for (int j = 0; j < 8; ++j)
                     if (w0 + j * blockDim.x < pairs) s2[w0 + j * blockDim.x] = v[j];
             }
-        } else {  // a one-word table
-            for (uint32_t w = tid; w < seg_words; w += blockDim.x) seg[w] = gseg[w];
+        } else {  // an odd number of words
+            for (uint32_t w = tid; w < words; w += blockDim.x) seg[w] = gseg[w];
         }
         __syncthreads();
         constexpr int U = 8;  // entries per thread in flight
@@ -581,8 +585,12 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
                       const uint64_t e = ev[j];
                       const uint32_t fp = static_cast<uint32_t>(e) & C::tag_mask;
                       uint64_t b = e >> C::bits;
-                      if (round == 1) b = alt_bucket<C>(b, fp, t.nb_mask);  // keyed by the alternate bucket
-                      next[o] = pack_entry<C>(b, fp);
+                      uint32_t tg = fp;
+                      if (round == 1) {  // keyed by the alternate bucket, the tag in that bucket's form
+                          b = alt_bucket<C>(b, fp, t.nb_mask);
+                          tg = alt_tag<C>(fp);
+                      }
+                      next[o] = pack_entry<C>(b, tg);
                       if (pay) next_pay[o] = pv[j];
                       ++o;
                   }
@@ -592,12 +600,12 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
         }
         __syncthreads();
         if constexpr (OP != SEG_CONTAINS) {
-            if (seg_words % 2 == 0) {
+            if (words % 2 == 0) {
                 ulonglong2* g2 = reinterpret_cast<ulonglong2*>(gseg);
                 const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(seg);
-                for (uint32_t w = tid; w < seg_words / 2; w += blockDim.x) __stcs(g2 + w, s2[w]);
+                for (uint32_t w = tid; w < words / 2; w += blockDim.x) __stcs(g2 + w, s2[w]);
             } else {
-                for (uint32_t w = tid; w < seg_words; w += blockDim.x) gseg[w] = seg[w];
+                for (uint32_t w = tid; w < words; w += blockDim.x) gseg[w] = seg[w];
             }
         }
         __syncthreads();
@@ -612,113 +620,6 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
             atomicAdd(&t.ctr[CTR_OCCUPIED], ~static_cast<unsigned long long>(s) + 1ull);
         }
     }
-    if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
-}
-
-// BFS for a list of keys whose two buckets were full (entries carry (alternate
-// bucket, tag)), eight lanes per key.  Lane j of a key's group reads candidate
-// j of the start bucket (slot (fp + 7j) & (bs-1)) and loads that candidate's
-// alternate bucket, so all candidates' buckets are fetched in one round trip;
-// the candidates with room are then tried in the reference's order
-// (CuckooFilter.cuh:967-1018): copy the candidate to its alternate bucket, swap
-// fp into its slot if it is still there, else undo the copy.  Keys whose
-// candidates all fail are appended to `dfs` for the DFS fallback.
-template <class C>
-__global__ void __launch_bounds__(256) k_evict_bfs_coop(DevTable t, const uint64_t* ent, const uint32_t* pay,
-                                                        const unsigned long long* n_dev, uint32_t* bitmap,
-                                                        uint64_t* dfs, uint32_t* dfs_pay,
-                                                        unsigned long long* dfs_count) {
-    constexpr uint32_t NC = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
-    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
-    const uint32_t lane = threadIdx.x & 31, gl = lane & 7, grp = lane >> 3;
-    const uint32_t gmask = 0xFFu << (grp * 8);
-    const uint64_t m = *n_dev;
-    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
-    const uint64_t wid = blockIdx.x * static_cast<uint64_t>(blockDim.x / 32) + threadIdx.x / 32;
-    uint32_t n_evk = 0, n_ok = 0, n_ev = 0, n_dup = 0;
-    bool err = false;
-    for (uint64_t i0 = wid * 4; i0 < m; i0 += nwarps * 4) {
-        const uint64_t i = i0 + grp;
-        const bool valid = i < m;
-        uint64_t e = 0, start = 0;
-        uint32_t fp = 0;
-        if (valid) {
-            e = ent[i];
-            fp = static_cast<uint32_t>(e) & C::tag_mask;
-            const uint64_t i2 = e >> C::bits;
-            const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
-            start = (fp & 1u) == 0 ? i1 : i2;
-        }
-        uint64_t* sbw = bucket_words<C>(t, start);
-        const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * gl) & (C::bs - 1));
-        const int sw = static_cast<int>(slot / C::lanes_per_chunk);
-        const int sh = static_cast<int>(slot % C::lanes_per_chunk) * C::bits;
-        uint32_t cand = 0;
-        uint64_t ab = 0;
-        bool room = false;
-        if (valid && gl < NC) {
-            uint64_t snap[C::nchunks];
-            load_rlx<C::bucket_bytes>(sbw, snap);
-            cand = static_cast<uint32_t>((pick(snap, sw) >> sh) & lane_mask);
-            if (cand == 0) {
-                room = true;  // an empty start slot: tryInsertAtBucket(start, fp), reference :980-985
-            } else {
-                ab = alt_bucket<C>(start, cand, t.nb_mask);
-                uint64_t c[C::nchunks];
-                load_rlx<C::bucket_bytes>(bucket_words<C>(t, ab), c);
-                uint64_t z = 0;
-#pragma unroll
-                for (int q = 0; q < C::nchunks; ++q) z |= zero_lanes<C::bits>(c[q]);
-                room = z != 0;
-            }
-        }
-        uint32_t todo = __ballot_sync(0xFFFFFFFFu, room) & gmask;
-        int done = 0;
-        while (todo) {  // candidates with room, lowest first (group-uniform)
-            const int leader = __ffs(todo) - 1;
-            int res = 0;
-            if (static_cast<int>(lane) == leader) {
-                uint64_t c[C::nchunks];
-                if (cand == 0) {
-                    load_rlx<C::bucket_bytes>(sbw, c);
-                    res = try_insert<C>(sbw, c, fp, err) ? 1 : 0;
-                } else {
-                    uint64_t* abw = bucket_words<C>(t, ab);
-                    load_rlx<C::bucket_bytes>(abw, c);
-                    if (try_insert<C>(abw, c, cand, err)) {
-                        const uint64_t word = load_word_rlx(sbw + sw);
-                        if (((word >> sh) & lane_mask) == cand) {
-                            const uint64_t desired = (word & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
-                            res = cas64(sbw + sw, word, desired) == word ? 2 : 0;
-                        }
-                        if (!res && !remove_from_pair<C>(t, ab, start, cand, err)) ++n_dup;
-                    }
-                }
-            }
-            res = __shfl_sync(gmask, res, leader);
-            if (res) {
-                done = res;
-                break;
-            }
-            todo &= ~(1u << leader);
-        }
-        if (valid && gl == 0) {
-            ++n_evk;
-            if (done) {
-                ++n_ok;
-                if (done == 2) ++n_ev;
-                if (bitmap) atomicOr(&bitmap[pay[i] >> 5], 1u << (pay[i] & 31));
-            } else {
-                const unsigned long long o = atomicAdd(dfs_count, 1ull);
-                dfs[o] = e;
-                if (dfs_pay) dfs_pay[o] = pay[i];
-            }
-        }
-    }
-    flush_counter(&t.ctr[CTR_OCCUPIED], n_ok + n_dup);
-    flush_counter(&t.ctr[CTR_DUP], n_dup);
-    flush_counter(&t.ctr[CTR_EVICTED_INSERTS], n_evk);
-    flush_counter(&t.ctr[CTR_EVICTIONS], n_ev);
     if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
 }
 
@@ -826,6 +727,7 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
                     const uint64_t i2 = e >> C::bits;
                     const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
                     start = (fp & 1u) == 0 ? i1 : i2;
+                    if ((fp & 1u) == 0) fp = alt_tag<C>(fp);  // the tag in the start bucket's form
                     phase = P_SNAP;
                     addr = bucket_words<C>(t, start);
                     break;
@@ -836,7 +738,7 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
                     outcome = select();
                     break;
                 case P_PROBE:
-                    if (plan_insert<C>(ld, cand, w, exp, des)) {
+                    if (plan_insert<C>(ld, alt_tag<C>(cand), w, exp, des)) {
                         phase = P_INS_ALT;
                         addr = bucket_words<C>(t, ab) + w;
                     } else {
@@ -865,7 +767,7 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
                         des = (old & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
                         if (++retries >= kCasRetryLimit) err = true;
                     } else {  // the candidate moved: undo the copy, refresh the snapshot
-                        if (!remove_from_pair<C>(t, ab, start, cand, err)) ++n_dup;
+                        if (!remove_from_pair<C>(t, ab, start, alt_tag<C>(cand), err)) ++n_dup;
                         ++i;
                         if (i == NC) {
                             outcome = 3;
@@ -938,10 +840,11 @@ __global__ void __launch_bounds__(256) k_evict_list(DevTable t, const uint64_t* 
         const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
         const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
         const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
+        const uint32_t sfp = (fp & 1u) == 0 ? alt_tag<C>(fp) : fp;  // the tag in the start bucket's form
         ++n_evk;
         const uint32_t before = st.evictions;
-        const bool ok = policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
-                                   : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+        const bool ok = policy_bfs ? evict_bfs<C>(t, sfp, start, other, max_ev, st, err)
+                                   : evict_dfs<C>(t, sfp, start, other, max_ev, st, err);
         if (ok) record_chain(t, st.evictions - before);
         if (ok) {
             if (bitmap) {
@@ -1023,10 +926,15 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
         const uint32_t lo = start[s], hi = start[s + 1];
         if (lo == hi) continue;
         uint64_t* gseg = reinterpret_cast<uint64_t*>(t.buckets + (s << sb_log2) * C::bucket_bytes);
-        if (seg_words % 2 == 0) {
+        // the last segment of a table whose bucket count is not a multiple of
+        // the segment (AddSub and Offset policies) is partial
+        const uint64_t left = t.nb_mask + 1 - (s << sb_log2);
+        const uint32_t nbk = left < sb ? static_cast<uint32_t>(left) : static_cast<uint32_t>(sb);
+        const uint32_t words = nbk * WPB;
+        if (words % 2 == 0) {
             const ulonglong2* g2 = reinterpret_cast<const ulonglong2*>(gseg);
             ulonglong2* s2 = reinterpret_cast<ulonglong2*>(seg);
-            const uint32_t pairs = seg_words / 2;
+            const uint32_t pairs = words / 2;
             for (uint32_t w0 = tid; w0 < pairs; w0 += blockDim.x * 8) {
                 ulonglong2 v[8];
 #pragma unroll
@@ -1037,10 +945,11 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                     if (w0 + j * blockDim.x < pairs) s2[w0 + j * blockDim.x] = v[j];
             }
         } else {
-            for (uint32_t w = tid; w < seg_words; w += blockDim.x) seg[w] = gseg[w];
+            for (uint32_t w = tid; w < words; w += blockDim.x) seg[w] = gseg[w];
         }
         __syncthreads();
-        for (uint32_t b = tid; b < sb; b += blockDim.x) mask[b] = empty_mask<C>(seg + static_cast<uint64_t>(b) * WPB);
+        for (uint32_t b = tid; b < sb; b += blockDim.x)
+            mask[b] = b < nbk ? empty_mask<C>(seg + static_cast<uint64_t>(b) * WPB) : static_cast<M>(0);
         __syncthreads();
         constexpr int U = 8;
         for (uint32_t base = lo; base < hi; base += blockDim.x * U) {
@@ -1117,8 +1026,12 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                     if ((fwd_mask >> j) & 1u) {
                         const uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
                         uint64_t b = ev[j] >> C::bits;
-                        if (round == 1) b = alt_bucket<C>(b, fp, t.nb_mask);
-                        next[o] = pack_entry<C>(b, fp);
+                        uint32_t tg = fp;
+                        if (round == 1) {  // keyed by the alternate bucket, the tag in that bucket's form
+                            b = alt_bucket<C>(b, fp, t.nb_mask);
+                            tg = alt_tag<C>(fp);
+                        }
+                        next[o] = pack_entry<C>(b, tg);
                         if constexpr (PAY) next_pay[o] = pv[j];
                         ++o;
                     }
@@ -1126,12 +1039,12 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
             }
             __syncthreads();
         }
-        if (seg_words % 2 == 0) {
+        if (words % 2 == 0) {
             ulonglong2* g2 = reinterpret_cast<ulonglong2*>(gseg);
             const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(seg);
-            for (uint32_t w = tid; w < seg_words / 2; w += blockDim.x) __stcs(g2 + w, s2[w]);
+            for (uint32_t w = tid; w < words / 2; w += blockDim.x) __stcs(g2 + w, s2[w]);
         } else {
-            for (uint32_t w = tid; w < seg_words; w += blockDim.x) gseg[w] = seg[w];
+            for (uint32_t w = tid; w < words; w += blockDim.x) gseg[w] = seg[w];
         }
         __syncthreads();
     }
@@ -1172,9 +1085,10 @@ __global__ void __launch_bounds__(256) k_list_random(DevTable t, const uint64_t*
                 const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
                 const uint64_t start = (fp & 1u) == 0 ? i1 : i2;
                 const uint64_t other = (fp & 1u) == 0 ? i2 : i1;
+                const uint32_t sfp = (fp & 1u) == 0 ? alt_tag<C>(fp) : fp;  // the tag in the start bucket's form
                 ++n_evk;
-                ok = policy_bfs ? evict_bfs<C>(t, fp, start, other, max_ev, st, err)
-                                : evict_dfs<C>(t, fp, start, other, max_ev, st, err);
+                ok = policy_bfs ? evict_bfs<C>(t, sfp, start, other, max_ev, st, err)
+                                : evict_dfs<C>(t, sfp, start, other, max_ev, st, err);
                 if (!ok) ++n_fail;
             }
         } else if constexpr (OP == SEG_DELETE) {

@@ -161,7 +161,54 @@ def test_bulk_invariants(cfb, orc, alt, policy, sorted_):
     f.close()
 
 
-def test_policies_reject_filter_sets(cfb, orc):
+def test_policies_reject_filter_sets(cfb, orc):  # noqa: D103
     cfg = cfb.CuckooConfig(T="uint64", bitsPerTag=16, bucketSize=16, AltBucketPolicy="OffsetAltBucketPolicy")
     with pytest.raises(cfb.CuckooError):
         cfb.CuckooFilterSet(cfg, [1 << 12, 1 << 12])
+
+
+@pytest.mark.parametrize("alt,policy,max_ev,fill", [(1, 1, 500, 0.97), (2, 0, 500, 0.97), (2, 1, 16, 1.0)])
+def test_sorted_insert_one_key_per_call_bit_exact(cfb, orc, alt, policy, max_ev, fill):
+    """insertManySorted (segment-staged: one partial segment, 253 buckets) one
+    key per call gives the oracle's image."""
+    f, o = make(cfb, orc, alt, policy=policy, max_ev=max_ev, cap=4048)
+    keys = orc.splitmix64(900 + alt * 10 + policy, int(fill * f.capacity()))
+    d = dev(keys)
+    out = torch.empty(1, dtype=torch.bool, device="cuda")
+    got = np.empty(len(keys), np.uint8)
+    for i in range(len(keys)):
+        f.insertManySorted(d[i:i + 1], d_output=out)
+        got[i] = int(out.item())
+    n_ok, want = o.insert(keys, out=True)
+    assert np.array_equal(got, want), f"first differing key {int(np.argmax(got != want))}"
+    assert np.array_equal(image(f), o.table)
+
+
+@pytest.mark.parametrize("alt", [1, 2])
+def test_segment_path_with_partial_last_segment(cfb, orc, alt):
+    """~62 500 buckets: 31 segments of 2048 buckets, the last one partial.
+    Segment-staged inserts, lookups and deletes keep every invariant and agree
+    with the random path on the same image."""
+    f, o = make(cfb, orc, alt, policy=0, cap=1_000_003)
+    assert o.nb % 2048 != 0
+    f.setOption(cfb.OPT_STAGING, 2)  # segment
+    keys = orc.splitmix64(31 + alt, int(0.95 * f.capacity()))
+    d = dev(keys)
+    ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
+    occ = f.insertMany(d, d_output=ok_t)
+    ok = host_u8(ok_t).astype(bool)
+    assert occ == ok.sum() == f.countOccupiedSlots() and f.stats()["lost"] == 0
+    slots = image(f).view(np.uint16).reshape(o.nb, 16)
+    stored = keys[ok]
+    i1, i2, fp = o.candidates(stored)
+    assert not orc.check_invariants(slots, o.alt_map(), i1, i2, fp, norm=o.pure_tag)
+    q = np.concatenate([stored, orc.splitmix64(77, 200_000)])
+    seg = host_u8(f.containsMany(dev(q)))
+    o.table[:] = image(f)
+    assert np.array_equal(seg, o.contains(q))
+    assert seg[: len(stored)].all()
+    half = len(stored) // 2
+    out = torch.empty(half, dtype=torch.bool, device="cuda")
+    occ1 = f.deleteMany(dev(stored[:half]), out)
+    assert host_u8(out).all() and occ1 == occ - half == f.countOccupiedSlots()
+    f.close()
