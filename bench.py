@@ -457,8 +457,10 @@ def run_b200(args, w: dict) -> dict | None:
     ops["contains"]["path"] = "segment-staged" if seg_q else "random probes"
     ops["delete"]["path"] = "segment-staged" if seg_d else "random probes"
 
-    # plain insertMany (random CAS path) on the same fill, timed on its own
+    # plain insertMany on the random CAS path (a fill this large would be
+    # segment-staged by default), on the same fill, timed on its own
     if sorted_fill and not args.no_plain:
+        f.setOption(cfb.OPT_STAGING, cfb.STAGING_RANDOM)
         ts = []
         for _ in range(max(1, min(args.steps, 3))):
             f.clear(stream)
@@ -473,6 +475,7 @@ def run_b200(args, w: dict) -> dict | None:
         ops["insert_plain"] = op(n_fill, ts, n_fill * 72 + 32 * (st_p["secondary"] + st_p["evicted_inserts"]))
         ops["insert_plain"]["path"] = "insertMany (random CAS), not part of the step"
         ops["insert_plain"]["failed"] = st_p["failed"]
+        f.setOption(cfb.OPT_STAGING, cfb.STAGING_AUTO)
     for name in ("insert", "contains", "delete"):
         tr = load_traffic(name, w, ops[name]["path"])
         if tr:
@@ -974,12 +977,15 @@ def run_grid(args) -> dict:
                     f.clear(stream)
                     f.resetEvictionCount()
                     e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                    # insertMany rows: the random CAS path (the default would stage this fill)
+                    f.setOption(cfb.OPT_STAGING, cfb.STAGING_RANDOM if path == "insertMany" else cfb.STAGING_AUTO)
                     e[0].record(stream)
                     if path == "insertMany":
                         f.insertManyAsync(fill, stream=stream)
                     else:
                         f.insertManySorted(fill, stream=stream)
                     e[1].record(stream)
+                    f.setOption(cfb.OPT_STAGING, cfb.STAGING_AUTO)
                     f.containsManyAsync(query, q_out, stream=stream)
                     e[2].record(stream)
                     f.deleteManyAsync(dele, stream=stream)
@@ -1005,20 +1011,24 @@ def run_grid(args) -> dict:
 # ------------------------------------------------------- alternate-bucket policies
 
 
-def _time_fill_query_delete(f, path, fill, query, dele, q_out, stream) -> dict:
-    """One cleared fill (insertMany or insertManySorted), lookups and deletes,
-    each timed with CUDA events on `stream`."""
+def _time_fill_query_delete(cfb, f, path, fill, query, dele, q_out, stream) -> dict:
+    """One cleared fill (insertMany on the random CAS path, or
+    insertManySorted), lookups and deletes, each timed with CUDA events on
+    `stream`."""
     import torch
 
     f.clear(stream)
     f.resetEvictionCount()
     e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    # a fill this large would be segment-staged by default: force random CAS
+    f.setOption(cfb.OPT_STAGING, cfb.STAGING_RANDOM if path == "insertMany" else cfb.STAGING_AUTO)
     e[0].record(stream)
     if path == "insertMany":
         f.insertManyAsync(fill, stream=stream)
     else:
         f.insertManySorted(fill, stream=stream)
     e[1].record(stream)
+    f.setOption(cfb.OPT_STAGING, cfb.STAGING_AUTO)
     f.containsManyAsync(query, q_out, stream=stream)
     e[2].record(stream)
     f.deleteManyAsync(dele, stream=stream)
@@ -1057,7 +1067,7 @@ def run_policies(args) -> dict:
         for path in ("insertMany", "insertManySorted"):
             res = {}
             for _ in range(2):  # the first pass warms the workspace and the caches
-                res = _time_fill_query_delete(f, path, fill, query, dele, q_out, stream)
+                res = _time_fill_query_delete(cfb, f, path, fill, query, dele, q_out, stream)
             res = {"policy": name, "insert_path": path, "num_buckets": f.getNumBuckets(),
                    "table_bytes": f.sizeInBytes(), **res}
             rows.append(res)

@@ -191,21 +191,22 @@ typedef enum cf_option {
     /* Upper bound on the device workspace of the segment-staged path, in bytes
      * (default 4 GiB).  Larger batches are processed in chunks that fit. */
     CF_OPT_WORKSPACE_LIMIT = 1,
-    /* Batch size from which containsMany/deleteMany (and the alternate-bucket
-     * round of every segment-staged batch) stream table segments through shared
-     * memory instead of probing at random.  0 = automatic (table bytes / 128 for
-     * lookups, / 64 for inserts and deletes); UINT64_MAX = never. */
+    /* Batch size from which insertMany, containsMany and deleteMany stream
+     * table segments through shared memory instead of probing at random
+     * (insertManySorted always does).  0 = automatic: one key per bucket for
+     * inserts, eight per bucket for lookups and deletes; UINT64_MAX = never. */
     CF_OPT_SEGMENTED_MIN_KEYS = 2,
     /* Read-only: bytes of workspace currently allocated. */
     CF_OPT_WORKSPACE_BYTES = 3,
     /* Inside a segment-staged batch: number of keys that missed their primary
      * bucket from which the alternate-bucket round is segment-staged too
-     * (otherwise those keys are probed at random).  0 = automatic, as above. */
+     * (otherwise those keys are probed at random).  0 = automatic (table bytes
+     * / 64 for inserts, eight keys per bucket for lookups and deletes). */
     CF_OPT_ROUND2_SEGMENTED_MIN_KEYS = 4,
     /* Batch size from which every operation is region-staged: the batch is
      * partitioned by ~16 MiB table region in one pass and applied region by
-     * region, so probes hit L2.  0 = automatic (table bytes / 128 keys for
-     * lookups, / 64 for inserts and deletes); UINT64_MAX = never. */
+     * region, so probes hit L2.  0 = automatic, which never picks this path
+     * (measured slower than the others on B200); UINT64_MAX = never. */
     CF_OPT_REGION_MIN_KEYS = 5,
     /* Force one execution path for every batch (cf_staging); CF_STAGING_AUTO
      * (default) picks by batch size as described above. */
@@ -239,7 +240,7 @@ int cf_get_chain_histogram(cf_filter* f, uint64_t* bins);
 /* Execution paths (CF_OPT_STAGING).  All give the same per-key results. */
 typedef enum cf_staging {
     CF_STAGING_AUTO = 0,
-    CF_STAGING_RANDOM = 1,  /* one probe per bucket at random (insertManySorted: segment-staged) */
+    CF_STAGING_RANDOM = 1,  /* probe buckets at random, any batch size (insertManySorted: segment-staged) */
     CF_STAGING_SEGMENT = 2, /* sort by 64 KiB segment, stage segments in shared memory */
     CF_STAGING_REGION = 3   /* partition by ~16 MiB region, apply in region order through L2 */
 } cf_staging;

@@ -221,3 +221,29 @@ def test_segmented_paths_agree_with_plain_paths(cfb, orc):
     force_segmented(cfb, f)
     seg = f.containsMany(q)
     assert torch.equal(plain, seg)
+
+
+def test_insertMany_stages_batches_of_at_least_one_key_per_bucket(cfb, orc):
+    """insertMany picks the segment path from one key per bucket on (many
+    launches per call) and probes at random below it (one launch); both keep
+    the invariants."""
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 18)  # 16384 buckets
+    nb = f.getNumBuckets()
+    keys = orc.splitmix64(44, int(0.9 * f.capacity()))
+    small, big = keys[: nb // 2], keys[nb // 2:]
+    c0 = cfb.launch_count()
+    f.insertMany(dev(small))
+    c1 = cfb.launch_count()
+    f.insertMany(dev(big))
+    c2 = cfb.launch_count()
+    assert c1 - c0 <= 2 and c2 - c1 >= 8, (c1 - c0, c2 - c1)
+    st = f.stats()
+    assert st["failed"] == 0 and st["lost"] == 0 and st["occupied"] == len(keys) == f.countOccupiedSlots()
+    assert not _stored_invariants(f, o, orc, keys)
+    assert host_u8(f.containsMany(dev(keys))).all()
+    # the option moves the threshold: never stage
+    f.clear()
+    f.setOption(cfb.OPT_SEGMENTED_MIN_KEYS, cfb.NEVER)
+    c3 = cfb.launch_count()
+    f.insertMany(dev(big))
+    assert cfb.launch_count() - c3 <= 2
