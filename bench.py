@@ -787,6 +787,7 @@ def run_served(args) -> dict:
         trace = srv.make_trace(tenants, load * 1e6, args.duration, seed=100 + i)
         server = srv.Server(cfb, tenants, hbm_budget_bytes=int(args.budget_gb * 1e9), max_wave_keys=1 << 24)
         try:
+            server.warm_up()
             served = server.run(trace)
             waves, launches = server.waves, server.launches
             admitted = len(server.admitted)

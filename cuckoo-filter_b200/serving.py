@@ -186,6 +186,23 @@ class Server:
         for s in self.sets.values():
             s.close()
 
+    def warm_up(self) -> None:
+        """Serve one throwaway key per (tag width, kind) and clear every table,
+        so that the first measured requests do not pay one-time costs (kernel
+        module loading, first use of the staging buffers).  The tables and the
+        wave counters are left as after construction."""
+        for bits in self.sets:
+            tid = next(t for t, (b, _) in self.slot.items() if b == bits)
+            for op in (OP_INSERT, OP_LOOKUP, OP_DELETE):
+                r = Request(rid=-1, tenant=tid, op=op, keys=np.array([12345], np.uint64), arrival=0.0)
+                ev, _ = self._launch_wave([r], 0)
+                ev.synchronize()
+        for st in self.sets.values():
+            st.clear(stream=self.stream)
+        self.torch.cuda.synchronize(self.dev)
+        self.waves = 0
+        self.launches = 0
+
     # -------------------------------------------------------------- waves
     def _form_wave(self, queues: dict) -> list[Request]:
         """Head run of same-kind requests of every tenant with pending work,
