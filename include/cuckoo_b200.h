@@ -47,8 +47,9 @@ typedef enum cf_eviction { CF_EVICT_BFS = 0, CF_EVICT_DFS = 1 } cf_eviction;
  * and OffsetAltBucketPolicy (:179-350; any bucket count, the tag's top bit is
  * a choice bit: 0 in the primary bucket, 1 in the alternate).  AddSub and
  * Offset are built for 16-bit tags in 16-slot buckets (the reference's
- * bucket_policy_benchmark.cu:16-17 geometry); their batches always take the
- * random-probe path. */
+ * bucket_policy_benchmark.cu:16-17 geometry); their batches take the
+ * random-probe or the segment-staged path (never the region-staged one), and
+ * filter sets take the XOR policy only. */
 typedef enum cf_alt_policy { CF_ALT_XOR = 0, CF_ALT_ADDSUB = 1, CF_ALT_OFFSET = 2 } cf_alt_policy;
 
 /*
