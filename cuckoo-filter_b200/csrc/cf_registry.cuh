@@ -229,7 +229,8 @@ struct Launchers {
     // the scatter keeps.  lo_bits >= 0 (the last pass; lo_bits == order_bits):
     // the histogram kernel also adds every item's segment into w.start.
     static cudaError_t rs_pass(bool keys_mode, bool payload, const DevTable& t, const void* src, int from, uint64_t n,
-                               int shift, int order_bits, int dst, const SegWork& w, cudaStream_t s, int lo_bits) {
+                               int shift, int order_bits, int dst, const SegWork& w, cudaStream_t s, int lo_bits,
+                               int narrow) {
         const int pay = !payload ? 0 : keys_mode ? 1 : 2;
         const int grid = w.rs_grid[pay];
         const int hgrid = grid * kRsHistSub;
@@ -253,13 +254,13 @@ struct Launchers {
         unsigned long long* err = t.ctr + CTR_ERROR;
         if (pay == 0)
             { k_rs_scatter<0><<<grid, kRsThreads, rs_scatter_smem<0>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
-                                                                          w.ent[dst], nullptr, err); CF_COUNT_LAUNCH(); }
+                                                                          w.ent[dst], nullptr, err, narrow); CF_COUNT_LAUNCH(); }
         else if (pay == 1)
             { k_rs_scatter<1><<<grid, kRsThreads, rs_scatter_smem<1>(), s>>>(ent_src, nullptr, n, nullptr, shift, order_bits, w.hist,
-                                                                          w.ent[dst], w.pay[dst], err); CF_COUNT_LAUNCH(); }
+                                                                          w.ent[dst], w.pay[dst], err, narrow); CF_COUNT_LAUNCH(); }
         else
             { k_rs_scatter<2><<<grid, kRsThreads, rs_scatter_smem<2>(), s>>>(ent_src, w.pay[from], n, nullptr, shift,
-                                                                          order_bits, w.hist, w.ent[dst], w.pay[dst], err); CF_COUNT_LAUNCH(); }
+                                                                          order_bits, w.hist, w.ent[dst], w.pay[dst], err, narrow); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
 
@@ -267,11 +268,15 @@ struct Launchers {
     // result.  keys_mode: the source is the key array; otherwise ent/pay[from].
     // Up to two passes, the last pass also counts the segments, and
     // *have_start tells that w.start then holds every segment's first index.
+    // Entries of the sorted result are 4-byte ((bucket within its segment) <<
+    // bits | tag) when the segment starts are counted (at most two passes)
+    // and that fits 32 bits; *narrow tells.
     static cudaError_t sort_by_segment(bool keys_mode, bool payload, const DevTable& t, const SegGeom& g,
                                        const SegWork& w, const void* keys, int from, uint64_t n, cudaStream_t s,
-                                       int* result, bool* have_start) {
+                                       int* result, bool* have_start, bool* narrow) {
         int cur = from;
         const bool count_segs = g.passes <= 2;
+        *narrow = count_segs && g.sb_log2 + C::bits <= 32;
         if (count_segs) {
             cudaError_t e = cudaMemsetAsync(w.start, 0, (g.nseg + 1) * sizeof(uint32_t), s);
             if (e != cudaSuccess) return e;
@@ -281,7 +286,8 @@ struct Launchers {
             const int dst = from_keys ? 0 : 1 - cur;
             const int lo_bits = count_segs && p == g.passes - 1 ? kRadixBits * p : -1;
             cudaError_t e = rs_pass(from_keys, payload, t, from_keys ? keys : nullptr, cur, n,
-                                    g.seg_shift + kRadixBits * p, kRadixBits * p, dst, w, s, lo_bits);
+                                    g.seg_shift + kRadixBits * p, kRadixBits * p, dst, w, s, lo_bits,
+                                    *narrow && p == g.passes - 1 ? 1 : 0);
             if (e != cudaSuccess) return e;
             cur = dst;
         }
@@ -293,7 +299,7 @@ struct Launchers {
 
     template <int OP>
     static cudaError_t seg_round(const DevTable& t, const SegGeom& g, const SegWork& w, int buf, bool payload,
-                                 int round, uint64_t n, bool have_start, cudaStream_t s) {
+                                 int round, uint64_t n, bool have_start, bool narrow, cudaStream_t s) {
         // the insert kernel stages a slot mask per bucket beside the segment
         constexpr int kMaxSmem = OP == SEG_INSERT ? kSegBytes + (kSegBytes / C::bucket_bytes) * sizeof(SlotMask<C>)
                                                   : kSegBytes;
@@ -317,7 +323,7 @@ struct Launchers {
         { (payload ? kern_pay : kern)<<<grid, threads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr,
                                                                      w.start, g.nseg, g.sb_log2, round, w.ent[other],
                                                                      payload ? w.pay[other] : nullptr, &w.cnt[round - 1],
-                                                                     payload ? w.bitmap : nullptr); CF_COUNT_LAUNCH(); }
+                                                                     payload ? w.bitmap : nullptr, narrow ? 1 : 0); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
 
@@ -328,9 +334,9 @@ struct Launchers {
         cudaError_t e = cudaMemsetAsync(w.cnt, 0, 4 * sizeof(unsigned long long), s);
         if (e == cudaSuccess && payload) e = cudaMemsetAsync(w.bitmap, 0, (m + 31) / 32 * 4, s);
         int a = 0;
-        bool have_start = false;
-        if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a, &have_start);
-        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, s);
+        bool have_start = false, narrow = false;
+        if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a, &have_start, &narrow);
+        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, narrow, s);
         // round 2: keys that missed their primary bucket, now in ent/pay[1 - a]
         if (e == cudaSuccess) e = cudaMemcpyAsync(w.h_cnt, w.cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -340,8 +346,8 @@ struct Launchers {
         if (m2 > 0) {
             if (m2 >= w.round2_segmented_min) {
                 int c = b;
-                e = sort_by_segment(false, payload, t, g, w, nullptr, b, m2, s, &c, &have_start);
-                if (e == cudaSuccess) e = seg_round<OP>(t, g, w, c, payload, 2, m2, have_start, s);
+                e = sort_by_segment(false, payload, t, g, w, nullptr, b, m2, s, &c, &have_start, &narrow);
+                if (e == cudaSuccess) e = seg_round<OP>(t, g, w, c, payload, 2, m2, have_start, narrow, s);
                 if (e == cudaSuccess && OP == SEG_INSERT) {
                     // keys whose two buckets are full: ent/pay[1 - c], count cnt[1]
                     uint32_t* bm = payload ? w.bitmap : nullptr;

@@ -276,7 +276,8 @@ __global__ void __launch_bounds__(kRsThreads, 2) k_rs_scatter(const uint64_t* __
                                                               const uint32_t* __restrict__ src_pay, uint64_t n,
                                                               const unsigned long long* n_dev, int shift, int lo_bits,
                                                               const uint32_t* offs, uint64_t* __restrict__ dst,
-                                                              uint32_t* __restrict__ dst_pay, unsigned long long* err) {
+                                                              uint32_t* __restrict__ dst_pay, unsigned long long* err,
+                                                              int narrow) {
     constexpr int IPT = rs_ipt<PAY>();
     constexpr int TILE = rs_tile<PAY>();
     extern __shared__ __align__(128) unsigned char rs_raw[];
@@ -434,7 +435,10 @@ __global__ void __launch_bounds__(kRsThreads, 2) k_rs_scatter(const uint64_t* __
             const uint64_t x = sm.in[b][q];
             const uint32_t d = static_cast<uint32_t>((x >> shift) & (kRadix - 1));
             const uint32_t g = sm.out_base[d] + q;
-            dst[g] = x;
+            if (narrow)  // the low 32 bits: (bucket within its segment) << bits | tag
+                reinterpret_cast<uint32_t*>(dst)[g] = static_cast<uint32_t>(x);
+            else
+                dst[g] = x;
             if constexpr (PAY) dst_pay[g] = sm.in_pay[b][q];
         }
         if (stable)
@@ -488,7 +492,7 @@ template <class C, int OP>
 __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                      const uint32_t* start, uint64_t nseg, int sb_log2, int round,
                                                      uint64_t* next, uint32_t* next_pay,
-                                                     unsigned long long* next_count, uint32_t* bitmap) {
+                                                     unsigned long long* next_count, uint32_t* bitmap, int narrow) {
     extern __shared__ __align__(16) uint64_t seg[];
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_base;
@@ -534,7 +538,7 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
               ev[j] = 0;
               pv[j] = 0;
               if (k < hi) {
-                  ev[j] = ent[k];
+                  ev[j] = narrow ? reinterpret_cast<const uint32_t*>(ent)[k] : ent[k];
                   if (pay) pv[j] = pay[k];
               }
           }
@@ -584,7 +588,8 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
                   if ((fwd_mask >> j) & 1u) {
                       const uint64_t e = ev[j];
                       const uint32_t fp = static_cast<uint32_t>(e) & C::tag_mask;
-                      uint64_t b = e >> C::bits;
+                      // the full bucket index from the segment (entries may be 4-byte)
+                      uint64_t b = (s << sb_log2) | ((e >> C::bits) & (sb - 1));
                       uint32_t tg = fp;
                       if (round == 1) {  // keyed by the alternate bucket, the tag in that bucket's form
                           b = alt_bucket<C>(b, fp, t.nb_mask);
@@ -907,7 +912,8 @@ template <class C, bool PAY>
 __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                             const uint32_t* start, uint64_t nseg, int sb_log2,
                                                             int round, uint64_t* next, uint32_t* next_pay,
-                                                            unsigned long long* next_count, uint32_t* bitmap) {
+                                                            unsigned long long* next_count, uint32_t* bitmap,
+                                                            int narrow) {
     using M = SlotMask<C>;
     extern __shared__ __align__(16) uint64_t seg[];
     __shared__ uint32_t s_warp[32];
@@ -961,7 +967,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                 ev[j] = 0;
                 if constexpr (PAY) pv[j] = 0;
                 if (k < hi) {
-                    ev[j] = ent[k];
+                    ev[j] = narrow ? reinterpret_cast<const uint32_t*>(ent)[k] : ent[k];
                     if constexpr (PAY) pv[j] = pay[k];
                 }
             }
@@ -1025,7 +1031,8 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                 for (int j = 0; j < U; ++j) {
                     if ((fwd_mask >> j) & 1u) {
                         const uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
-                        uint64_t b = ev[j] >> C::bits;
+                        // the full bucket index from the segment (entries may be 4-byte)
+                        uint64_t b = (s << sb_log2) | ((ev[j] >> C::bits) & (sb - 1));
                         uint32_t tg = fp;
                         if (round == 1) {  // keyed by the alternate bucket, the tag in that bucket's form
                             b = alt_bucket<C>(b, fp, t.nb_mask);
