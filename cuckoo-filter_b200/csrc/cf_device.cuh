@@ -129,7 +129,8 @@ struct Cfg {
     static_assert(WB == 4 || WB == 8, "WordType is uint32_t or uint64_t");
     static_assert(BITS <= WB * 8, "a tag must fit in one word");
     static_assert(BS % tpw == 0, "bucket size must be a multiple of tags per word");
-    static_assert(BS <= 64, "at most 64 slots per bucket");
+    static_assert(BS <= 128, "at most 128 slots per bucket");
+    static_assert(nchunks <= 32, "at most 32 chunks (256 bytes) per bucket");
     static_assert(POL == ALT_XOR || POL == ALT_ADDSUB || POL == ALT_OFFSET, "alternate-bucket policy");
     using Key = typename std::conditional<KB == 8, uint64_t, uint32_t>::type;
 };

@@ -96,8 +96,8 @@ __device__ __forceinline__ int first_word(uint32_t words, int sw) {
     if constexpr (WC == 1) {
         return 0;
     } else {
-        const uint32_t full = (1u << WC) - 1u;
-        const uint32_t rot = ((words >> sw) | (words << (WC - sw))) & full;
+        constexpr uint32_t full = WC == 32 ? ~0u : ((1u << (WC % 32)) - 1u);
+        const uint32_t rot = sw ? (((words >> sw) | (words << (WC - sw))) & full) : words;
         return (sw + __ffs(rot) - 1) & (WC - 1);
     }
 }
@@ -109,6 +109,7 @@ using SlotMask = typename std::conditional<(C::bs > 32), unsigned long long, uns
 // Bit s set when slot s of bucket image c holds `tag` (0: the empty slots).
 template <class C>
 __device__ __forceinline__ SlotMask<C> slots_holding(const uint64_t (&c)[C::nchunks], uint32_t tag) {
+    static_assert(C::bs <= 64, "slot masks hold at most 64 slots");
     const uint64_t rep = replicate<C::bits>(tag);
     SlotMask<C> m = 0;
 #pragma unroll

@@ -160,7 +160,7 @@ struct Launchers {
     using Key = typename C::Key;
     // keys per thread; buckets wider than 64 bytes keep fewer in flight so
     // their images stay in registers
-    static constexpr int CKPT = C::bucket_bytes > 64 ? 2 : kContainsKPT;
+    static constexpr int CKPT = C::bucket_bytes > 128 ? 1 : C::bucket_bytes > 64 ? 2 : kContainsKPT;
     static constexpr int DKPT = C::bucket_bytes > 64 ? 1 : kDeleteKPT;
     static constexpr int IKPT = C::bucket_bytes > 64 ? 1 : kInsertKPT;
 
@@ -300,13 +300,21 @@ struct Launchers {
     template <int OP>
     static cudaError_t seg_round(const DevTable& t, const SegGeom& g, const SegWork& w, int buf, bool payload,
                                  int round, uint64_t n, bool have_start, bool narrow, cudaStream_t s) {
-        // the insert kernel stages a slot mask per bucket beside the segment
-        constexpr int kMaxSmem = OP == SEG_INSERT ? kSegBytes + (kSegBytes / C::bucket_bytes) * sizeof(SlotMask<C>)
-                                                  : kSegBytes;
-        constexpr auto kern = OP == SEG_INSERT ? k_seg_insert<C, false> : k_seg<C, OP>;
-        constexpr auto kern_pay = OP == SEG_INSERT ? k_seg_insert<C, true> : k_seg<C, OP>;
-        const int smem = static_cast<int>(OP == SEG_INSERT ? seg_insert_smem<C>(g.sb_log2)
-                                                           : (1ull << g.sb_log2) * C::bucket_bytes);
+        // inserts claim slots on a per-bucket mask of at most 64 bits, staged
+        // beside the segment; buckets of more slots insert with
+        // compare-and-swap on the staged words
+        constexpr bool masked = OP == SEG_INSERT && C::bs <= 64;
+        constexpr int kMaxSmem = masked ? kSegBytes + (kSegBytes / C::bucket_bytes) * sizeof(SlotMask<C>) : kSegBytes;
+        constexpr auto kern = [] {
+            if constexpr (masked) return k_seg_insert<C, false>;
+            else return k_seg<C, OP>;
+        }();
+        constexpr auto kern_pay = [] {
+            if constexpr (masked) return k_seg_insert<C, true>;
+            else return k_seg<C, OP>;
+        }();
+        const int smem = static_cast<int>(masked ? seg_insert_smem<C>(g.sb_log2)
+                                                 : (1ull << g.sb_log2) * C::bucket_bytes);
         cudaError_t e = ensure_smem_attr<kern>(kMaxSmem);
         if (e == cudaSuccess) e = ensure_smem_attr<kern_pay>(kMaxSmem);
         if (e != cudaSuccess) return e;
@@ -319,7 +327,7 @@ struct Launchers {
         // one CTA per segment (measured faster on B200 than one wave of CTAs
         // striding over the segments)
         const int grid = static_cast<int>(g.nseg < 0x7FFFFFFFull ? g.nseg : 0x7FFFFFFFull);
-        const int threads = OP == SEG_INSERT ? kSegInsertThreads : kSegThreads;
+        const int threads = masked ? kSegInsertThreads : kSegThreads;
         { (payload ? kern_pay : kern)<<<grid, threads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr,
                                                                      w.start, g.nseg, g.sb_log2, round, w.ent[other],
                                                                      payload ? w.pay[other] : nullptr, &w.cnt[round - 1],

@@ -878,6 +878,7 @@ constexpr size_t seg_insert_smem(int sb_log2) {
 // Empty-slot mask of a bucket image (bit s set when slot s holds 0).
 template <class C>
 __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
+    static_assert(C::bs <= 64, "slot masks hold at most 64 slots");
     SlotMask<C> m = 0;
 #pragma unroll
     for (int j = 0; j < C::nchunks; ++j) {

@@ -60,7 +60,7 @@ typedef enum cf_alt_policy { CF_ALT_XOR = 0, CF_ALT_ADDSUB = 1, CF_ALT_OFFSET = 
 typedef struct cf_config {
     uint32_t key_bytes;       /* sizeof(T): 4 (uint32_t) or 8 (uint64_t) */
     uint32_t bits_per_tag;    /* bitsPerTag: 8, 16 or 32 */
-    uint32_t bucket_size;     /* bucketSize: slots per bucket, power of two, 8..128 bytes per bucket */
+    uint32_t bucket_size;     /* bucketSize: slots per bucket, power of two, 8..256 bytes per bucket */
     uint32_t word_bytes;      /* sizeof(WordType): 8, or 4 for the (8, 16), (16, 16) and (32, 8) tag/bucket geometries */
     uint32_t eviction_policy; /* cf_eviction */
     uint32_t max_evictions;   /* maxEvictions: 1..512 */

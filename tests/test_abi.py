@@ -102,12 +102,12 @@ def _cfg(cfb, **kw):
 
 def test_config_support_matrix(cfb):
     L = cfb.library()
-    for bits, sizes in ((8, (8, 16, 32, 64)), (16, (4, 8, 16, 32, 64)), (32, (2, 4, 8, 16))):
+    for bits, sizes in ((8, (8, 16, 32, 64)), (16, (4, 8, 16, 32, 64, 128)), (32, (2, 4, 8, 16))):
         for bs in sizes:
             for t in ("uint64", "uint32"):
                 assert L.cf_config_supported(C.byref(_cfg(cfb, T=t, bitsPerTag=bits, bucketSize=bs)))
     assert not L.cf_config_supported(C.byref(_cfg(cfb, bitsPerTag=8, bucketSize=4)))
-    assert not L.cf_config_supported(C.byref(_cfg(cfb, bitsPerTag=16, bucketSize=128)))
+    assert not L.cf_config_supported(C.byref(_cfg(cfb, bitsPerTag=16, bucketSize=256)))
     assert not L.cf_config_supported(C.byref(_cfg(cfb, bitsPerTag=32, bucketSize=32)))
 
 
@@ -117,7 +117,7 @@ def test_config_support_matrix(cfb):
     (dict(maxEvictions=0), -1),
     (dict(maxEvictions=513), -1),
     (dict(blockSize=100), -1),
-    (dict(bitsPerTag=16, bucketSize=128), -2),
+    (dict(bitsPerTag=16, bucketSize=256), -2),
 ])
 def test_create_rejects_bad_configs(cfb, kw, status):
     L = cfb.library()

@@ -78,6 +78,7 @@ SEQ_CASES = [
     (8, 8, 64, 1, 64, 1 << 12, 0.99),
     (8, 16, 64, 1, 500, 1 << 12, 0.97),  # 128-byte buckets
     (8, 16, 64, 0, 16, 1 << 12, 1.00),
+    (8, 16, 128, 1, 500, 1 << 12, 0.97),  # 256-byte buckets
 ]
 
 
@@ -150,7 +151,7 @@ def _ref_image(cfb, ref, kb, bits, bs) -> np.ndarray:
 
 
 LOOKUP_CASES = [(8, 16, 16), (8, 8, 16), (8, 32, 8), (4, 16, 16), (8, 16, 4), (8, 8, 64), (8, 16, 32), (4, 32, 16),
-                (8, 16, 64)]
+                (8, 16, 64), (8, 16, 128), (4, 16, 128)]
 
 
 @pytest.mark.parametrize("kb,bits,bs", LOOKUP_CASES)
@@ -206,7 +207,7 @@ def _stored_invariants(f, o, orc, stored_keys):
 
 
 BULK_CASES = [(8, 16, 16, 0), (8, 16, 16, 1), (8, 8, 16, 0), (8, 32, 8, 1), (8, 32, 8, 0), (4, 16, 16, 1),
-              (8, 16, 64, 0)]
+              (8, 16, 64, 0), (8, 16, 128, 1), (4, 16, 128, 0)]
 
 
 @pytest.mark.parametrize("staging", ["random", "region"])

@@ -37,6 +37,7 @@ SEQ = [
     (8, 8, 16, 0, 500, 1 << 12, 0.97),
     (4, 16, 16, 1, 500, 1 << 12, 0.97),
     (8, 16, 64, 1, 500, 1 << 12, 0.97),
+    (8, 16, 128, 0, 500, 1 << 12, 0.97),
 ]
 
 
@@ -61,7 +62,7 @@ def test_sorted_insert_one_key_per_call_bit_exact(cfb, orc, kb, bits, bs, policy
 BULK = [(8, 16, 16, 0, 1 << 20, 0.95), (8, 16, 16, 1, 1 << 20, 0.95), (8, 8, 16, 0, 1 << 20, 0.95),
         (8, 32, 8, 1, 1 << 20, 0.95), (8, 32, 8, 0, 1 << 20, 0.95), (4, 16, 16, 1, 1 << 20, 0.95),
         (8, 16, 16, 0, 1 << 24, 0.95), (8, 8, 64, 0, 1 << 20, 0.95), (8, 32, 2, 0, 1 << 18, 0.80),
-        (8, 16, 4, 1, 1 << 16, 0.90), (8, 16, 64, 1, 1 << 20, 0.95)]
+        (8, 16, 4, 1, 1 << 16, 0.90), (8, 16, 64, 1, 1 << 20, 0.95), (8, 16, 128, 0, 1 << 20, 0.95)]
 
 
 @pytest.mark.parametrize("kb,bits,bs,policy,cap,fill", BULK)
