@@ -35,7 +35,7 @@ struct cf_filter {
     int sms;
     // segment-staged path
     bool seg_ok;            // the segment-staged path applies: packed (bucket, tag) entries fit in 64 bits
-    bool rg_ok;             // the region-staged path applies (XOR policy)
+    bool rg_ok;             // the region-staged path applies
     SegGeom geom;
     void* ws;               // workspace (grown on demand, freed with the filter)
     uint64_t ws_bytes;
@@ -213,14 +213,16 @@ void init_geometry(cf_filter* f) {
     // (bucket << bits) | tag must fit in 64 bits for every bucket index
     f->seg_ok = clog2(f->num_buckets) + static_cast<int>(f->cfg.bits_per_tag) <= 64 && f->ops->seg_chunk;
     f->rg_ok = f->seg_ok && f->ops->rg_chunk;
-    // regions of ~kRgRegionBytes (or CF_OPT_REGION_BYTES), at most kRgMaxRegions of them
-    const int nb_log2 = ilog2(f->num_buckets);
+    // regions of ~kRgRegionBytes (or CF_OPT_REGION_BYTES), at most kRgMaxRegions
+    // of them; the last region is partial when the bucket count is not a power
+    // of two (AddSub and Offset policies)
+    const int nb_log2 = clog2(f->num_buckets);
     const uint64_t rbytes = f->rg_bytes ? f->rg_bytes : kRgRegionBytes;
     int rl = rbytes > bb ? ilog2(rbytes / bb) : 0;
     if (rl < nb_log2 - 8) rl = nb_log2 - 8;
     if (rl > nb_log2) rl = nb_log2;
     f->rgeom.rl = rl;
-    f->rgeom.nreg = static_cast<uint32_t>(f->num_buckets >> rl);
+    f->rgeom.nreg = static_cast<uint32_t>(((f->num_buckets - 1) >> rl) + 1);
 }
 
 // Bytes of workspace for a chunk of `cap` keys: two entry buffers (8 B per
@@ -431,7 +433,9 @@ namespace cfb {
 int api_fail(int status, const char* msg) { return fail(status, "%s", msg); }
 int api_cuda_fail(cudaError_t e, const char* what) { return cuda_fail(e, what); }
 int api_validate(const cf_config* cfg) { return validate(cfg); }
-uint64_t api_num_buckets(uint64_t capacity, uint32_t bucket_size) { return num_buckets_for(capacity, bucket_size); }
+uint64_t api_num_buckets(uint64_t capacity, uint32_t bucket_size, uint32_t alt_policy) {
+    return num_buckets_policy(capacity, bucket_size, alt_policy);
+}
 }  // namespace cfb
 
 extern "C" {

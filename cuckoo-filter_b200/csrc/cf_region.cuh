@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rg_scatter(const void* src, c
                 uint32_t fp;
                 candidates<C>(x[j], nb_mask, i1, fp);
                 e[j * EPI] = pack_entry<C>(i1, fp);
-                if constexpr (MODE == RG_KEYS_DUAL) e[j * EPI + 1] = pack_entry<C>(alt_bucket<C>(i1, fp, nb_mask), fp);
+                if constexpr (MODE == RG_KEYS_DUAL)  // the alternate bucket with the tag in that bucket's form
+                    e[j * EPI + 1] = pack_entry<C>(alt_bucket<C>(i1, fp, nb_mask), alt_tag<C>(fp));
             }
 #pragma unroll
             for (int k = 0; k < EPI; ++k) {
@@ -320,9 +321,12 @@ __global__ void __launch_bounds__(kRgThreads) k_rg_probe(DevTable t, const uint6
 #pragma unroll
                 for (int j = 0; j < U; ++j) {
                     if ((fwd_mask >> j) & 1u) {
-                        const uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
+                        uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
                         uint64_t b = ev[j] >> C::bits;
-                        if (round == 1) b = alt_bucket<C>(b, fp, t.nb_mask);
+                        if (round == 1) {  // keyed by the alternate bucket, the tag in that bucket's form
+                            b = alt_bucket<C>(b, fp, t.nb_mask);
+                            fp = alt_tag<C>(fp);
+                        }
                         next[o] = pack_entry<C>(b, fp);
                         if (next_pay) next_pay[o] = pv[j];
                         ++o;

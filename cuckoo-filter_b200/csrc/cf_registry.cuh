@@ -508,8 +508,7 @@ struct Launchers {
         o.probe = probe;
         o.occupancy = occupancy;
         o.seg_chunk = seg_chunk;
-        // the region-staged path is kept for the XOR policy only
-        if constexpr (C::alt_policy == ALT_XOR) o.rg_chunk = rg_chunk;
+        o.rg_chunk = rg_chunk;
         return o;
     }
 };

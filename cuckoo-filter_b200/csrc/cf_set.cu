@@ -22,7 +22,7 @@ namespace cfb {
 int api_fail(int status, const char* msg);
 int api_cuda_fail(cudaError_t e, const char* what);
 int api_validate(const cf_config* cfg);
-uint64_t api_num_buckets(uint64_t capacity, uint32_t bucket_size);
+uint64_t api_num_buckets(uint64_t capacity, uint32_t bucket_size, uint32_t alt_policy);
 }  // namespace cfb
 
 using namespace cfb;
@@ -36,7 +36,7 @@ struct LaunchChoice {
 // Launchers of one configuration, dispatching the runtime (kpt, width) to the
 // compiled variants.
 struct SetOps {
-    uint32_t bits, bucket_size, bucket_bytes;
+    uint32_t bits, bucket_size, bucket_bytes, alt_policy;
     cudaError_t (*contains)(const DevTable*, const uint32_t*, const uint64_t*, uint32_t, uint32_t, const void*, uint64_t,
                             uint8_t*, unsigned long long*, const LaunchChoice&, int sms, cudaStream_t);
     cudaError_t (*remove)(const DevTable*, const uint32_t*, const uint64_t*, uint32_t, uint32_t, const void*, uint64_t,
@@ -154,23 +154,26 @@ struct SetLaunch {
         }
     }
     static SetOps table() {
-        return SetOps{C::bits, C::bs, C::bucket_bytes, contains, remove, insert, width_ok};
+        return SetOps{C::bits, C::bs, C::bucket_bytes, C::alt_policy, contains, remove, insert, width_ok};
     }
 };
 
 // Set configurations: 64-bit keys with 8-bit tags in 16-slot buckets, 16-bit
 // tags in 16-slot buckets, 32-bit tags in 8-slot buckets (one 16- or 32-byte
-// bucket per sector).
+// bucket per sector), XOR policy; 16/16 also with the AddSub and Offset
+// policies.
 const std::vector<SetOps>& set_registry() {
-    static const std::vector<SetOps> v = {SetLaunch<Cfg<8, 8, 16, 8>>::table(), SetLaunch<Cfg<8, 16, 16, 8>>::table(),
-                                          SetLaunch<Cfg<8, 32, 8, 8>>::table()};
+    static const std::vector<SetOps> v = {
+        SetLaunch<Cfg<8, 8, 16, 8>>::table(), SetLaunch<Cfg<8, 16, 16, 8>>::table(),
+        SetLaunch<Cfg<8, 32, 8, 8>>::table(), SetLaunch<Cfg<8, 16, 16, 8, ALT_ADDSUB>>::table(),
+        SetLaunch<Cfg<8, 16, 16, 8, ALT_OFFSET>>::table()};
     return v;
 }
 
 const SetOps* find_set_ops(const cf_config* c) {
-    if (c->key_bytes != 8 || c->word_bytes != 8 || c->alt_policy != CF_ALT_XOR) return nullptr;
+    if (c->key_bytes != 8 || c->word_bytes != 8) return nullptr;
     for (const SetOps& o : set_registry())
-        if (o.bits == c->bits_per_tag && o.bucket_size == c->bucket_size) return &o;
+        if (o.bits == c->bits_per_tag && o.bucket_size == c->bucket_size && o.alt_policy == c->alt_policy) return &o;
     return nullptr;
 }
 
@@ -232,7 +235,8 @@ int cf_set_create(const cf_config* cfg, uint32_t n_filters, const uint64_t* capa
     const SetOps* ops = find_set_ops(cfg);
     if (!ops)
         return api_fail(CF_ERR_UNSUPPORTED,
-                        "filter sets are built for 64-bit keys with 8/16, 16/16 or 32/8 (bits per tag / bucket size)");
+                        "filter sets are built for 64-bit keys with 8/16, 16/16 or 32/8 (bits per tag / bucket size) "
+                        "and the XOR policy, and 16/16 with the AddSub and Offset policies");
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return api_fail(CF_ERR_NOT_LOADED, "no CUDA device");
     cf_set* s = new cf_set{};
@@ -248,7 +252,7 @@ int cf_set_create(const cf_config* cfg, uint32_t n_filters, const uint64_t* capa
             delete s;
             return api_fail(CF_ERR_INVALID, "every capacity must be > 0");
         }
-        s->nb[i] = api_num_buckets(capacities[i], cfg->bucket_size);
+        s->nb[i] = api_num_buckets(capacities[i], cfg->bucket_size, cfg->alt_policy);
         s->offset[i] = total;
         total += (s->nb[i] * ops->bucket_bytes + 255) & ~255ull;  // 256-byte aligned tables
     }

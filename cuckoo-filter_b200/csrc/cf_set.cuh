@@ -136,6 +136,7 @@ __global__ void __launch_bounds__(512) k_set_contains1(const DevTable* __restric
         for (int j = 0; j < KPT; ++j) {
             if (((valid >> j) & 1u) && !((hit >> j) & 1u)) {
                 b[j] = alt_bucket<C>(b[j], fp[j], t[j].nb_mask);
+                fp[j] = alt_tag<C>(fp[j]);  // the tag in the alternate bucket's form
                 load_nc<C::bucket_bytes>(t[j].buckets + b[j] * C::bucket_bytes, c[j]);
             }
         }
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(512) k_set_containsW(const DevTable* __restric
         for (int j = 0; j < KPT; ++j) {
             if (((valid >> j) & 1u) && !((hit >> j) & 1u)) {
                 b[j] = alt_bucket<C>(b[j], fp[j], t[j].nb_mask);
+                fp[j] = alt_tag<C>(fp[j]);
                 piece[j] = load_piece<PB>(t[j].buckets + b[j] * C::bucket_bytes + r * PB);
             }
         }
@@ -252,6 +254,7 @@ __global__ void __launch_bounds__(512) k_set_delete(const DevTable* __restrict__
                 ok = try_remove<C>(bucket_words<C>(t, b), c, fp, err);
                 if (!ok && !err) {
                     b = alt_bucket<C>(b, fp, t.nb_mask);
+                    fp = alt_tag<C>(fp);
                     load_rlx<C::bucket_bytes>(t.buckets + b * C::bucket_bytes, c);
                     ok = try_remove<C>(bucket_words<C>(t, b), c, fp, err);
                 }
@@ -332,6 +335,7 @@ __global__ void __launch_bounds__(512) k_set_insert(const DevTable* __restrict__
                     where = 1;
                 } else if (!err) {
                     b = alt_bucket<C>(b, fp, t.nb_mask);
+                    fp = alt_tag<C>(fp);
                     load_rlx<C::bucket_bytes>(t.buckets + b * C::bucket_bytes, c);
                     if (try_insert<C>(bucket_words<C>(t, b), c, fp, err)) where = 2;
                 }

@@ -47,9 +47,8 @@ typedef enum cf_eviction { CF_EVICT_BFS = 0, CF_EVICT_DFS = 1 } cf_eviction;
  * and OffsetAltBucketPolicy (:179-350; any bucket count, the tag's top bit is
  * a choice bit: 0 in the primary bucket, 1 in the alternate).  AddSub and
  * Offset are built for 16-bit tags in 16-slot buckets (the reference's
- * bucket_policy_benchmark.cu:16-17 geometry); their batches take the
- * random-probe or the segment-staged path (never the region-staged one), and
- * filter sets take the XOR policy only. */
+ * bucket_policy_benchmark.cu:16-17 geometry), on every execution path and in
+ * filter sets. */
 typedef enum cf_alt_policy { CF_ALT_XOR = 0, CF_ALT_ADDSUB = 1, CF_ALT_OFFSET = 2 } cf_alt_policy;
 
 /*
@@ -313,7 +312,8 @@ int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* prima
  * Batched form over many filters (an extension; the reference runs one filter
  * per object and one launch per batch, CuckooFilter.cuh:457-548).  A set holds
  * n_filters independent filters of one configuration (64-bit keys; 8/16, 16/16
- * or 32/8 bits per tag / bucket size), each with its own capacity and its own
+ * or 32/8 bits per tag / bucket size with the XOR policy, 16/16 with AddSub or
+ * Offset), each with its own capacity and its own
  * counters, tables in one device pool.  A batched call takes a device work
  * list: item j covers keys [d_offsets[j], d_offsets[j+1]) of the concatenated
  * key buffer and targets filter d_filters[j]; d_offsets has n_items + 1

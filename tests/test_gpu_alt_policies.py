@@ -6,7 +6,8 @@ Exact checks against the oracle: one-key-per-call insert images (evictions,
 failed chains and their undo included), lookups on identical images, one-key
 deletes.  The oracle's policy code is pinned to the reference's own kernels
 built with these policies.  Bulk batches are checked through invariants (the
-Offset policy's choice bit is set exactly on tags in their alternate bucket).
+Offset policy's choice bit is set exactly on tags in their alternate bucket),
+on the random, segment- and region-staged paths and in filter sets.
 """
 from __future__ import annotations
 
@@ -161,10 +162,97 @@ def test_bulk_invariants(cfb, orc, alt, policy, sorted_):
     f.close()
 
 
-def test_policies_reject_filter_sets(cfb, orc):  # noqa: D103
-    cfg = cfb.CuckooConfig(T="uint64", bitsPerTag=16, bucketSize=16, AltBucketPolicy="OffsetAltBucketPolicy")
-    with pytest.raises(cfb.CuckooError):
-        cfb.CuckooFilterSet(cfg, [1 << 12, 1 << 12])
+def make_set(cfb, orc, alt, caps):
+    cfg = cfb.CuckooConfig(T="uint64", bitsPerTag=16, bucketSize=16, AltBucketPolicy=NAMES[alt])
+    s = cfb.CuckooFilterSet(cfg, caps)
+    oracles = [orc.OracleFilter(key_bytes=8, bits=16, bucket_size=16, policy=1, max_evictions=500, capacity=int(c),
+                                mode=orc.MODE_CONSERVING, alt_policy=alt) for c in caps]
+    for i, o in enumerate(oracles):
+        assert s.num_buckets[i] == o.nb == cfb.CuckooFilter.calculateNumBuckets(int(caps[i]), 16, NAMES[alt])
+    return s, oracles
+
+
+def set_work(batches):
+    keys = np.concatenate([k for _, k in batches])
+    offs = np.zeros(len(batches) + 1, np.int64)
+    offs[1:] = np.cumsum([len(k) for _, k in batches])
+    filt = np.array([f for f, _ in batches], np.int32)
+    return dev(keys), torch.from_numpy(offs).cuda(), torch.from_numpy(filt).cuda(), keys
+
+
+def set_caps(alt):
+    # bucket counts that are not powers of two (AddSub: even; Offset: any)
+    rng = np.random.default_rng(70 + alt)
+    return (16 * rng.integers(300, 5000, 12) + 16 * 3).astype(np.uint64)
+
+
+@pytest.mark.parametrize("alt", [1, 2])
+def test_set_lookups_and_deletes_on_identical_images(cfb, orc, alt):
+    """Filter sets with the policy: lookups on images the oracle built equal the
+    oracle's, for every probe width; batched deletes remove one copy per key."""
+    s, oracles = make_set(cfb, orc, alt, set_caps(alt))
+    batches, stored = [], []
+    for i, o in enumerate(oracles):
+        keys = orc.splitmix64(600 + 10 * alt + i, int(0.9 * o.nb * 16))
+        o.insert(keys)
+        s.load_table(i, torch.from_numpy(o.table))
+        stored.append(keys)
+        q = np.concatenate([keys[:700], orc.splitmix64(7000 + i, 500)])
+        batches += [(i, q[:300]), (i, q[300:])]
+    d_keys, d_offs, d_filt, h_keys = set_work(batches)
+    want = np.concatenate([oracles[i].contains(q) for i, q in batches])
+    for kpt in (1, 4):
+        for w in (1, 4, 8):
+            s.set_launch(cfb.SET_CONTAINS, 256, kpt, w)
+            out = torch.full((len(h_keys),), 7, dtype=torch.uint8, device="cuda")
+            s.contains_async(d_keys, d_offs, d_filt, out)
+            s.sync()
+            assert np.array_equal(host_u8(out), want), (kpt, w)
+    s.clear()
+    for i, o in enumerate(oracles):
+        s.load_table(i, torch.from_numpy(o.table))
+    dels = [(i, k[: len(k) // 2]) for i, k in enumerate(stored)]
+    dk, do, df, dh = set_work(dels)
+    out = torch.zeros(len(dh), dtype=torch.uint8, device="cuda")
+    s.delete_async(dk, do, df, out)
+    s.sync()
+    assert host_u8(out).all(), "a stored key was not deleted"
+    for i, o in enumerate(oracles):
+        o.delete(dels[i][1])
+        slots = s.table_image(i).numpy().view(np.uint16).reshape(o.nb, 16)
+        assert int((slots != 0).sum()) == o.occupied()
+        rest = stored[i][len(stored[i]) // 2:]
+        i1, i2, fp = o.candidates(rest)
+        assert not orc.check_invariants(slots, o.alt_map(), i1, i2, fp, norm=o.pure_tag), i
+
+
+@pytest.mark.parametrize("alt", [1, 2])
+def test_set_inserts_keep_every_filter_invariant(cfb, orc, alt):
+    s, oracles = make_set(cfb, orc, alt, set_caps(alt))
+    batches, per_filter = [], []
+    for i, o in enumerate(oracles):
+        keys = orc.splitmix64(650 + 10 * alt + i, int(0.9 * o.nb * 16))
+        per_filter.append(keys)
+        half = len(keys) // 2
+        batches += [(i, keys[:half]), (i, keys[half:])]
+    np.random.default_rng(alt).shuffle(batches)
+    d_keys, d_offs, d_filt, h_keys = set_work(batches)
+    ok = torch.zeros(len(h_keys), dtype=torch.uint8, device="cuda")
+    s.insert_async(d_keys, d_offs, d_filt, ok)
+    s.sync()
+    assert host_u8(ok).all()
+    occ = s.occupied()
+    for i, o in enumerate(oracles):
+        st = s.stats(i)
+        slots = s.table_image(i).numpy().view(np.uint16).reshape(o.nb, 16)
+        assert st["lost"] == 0 and st["failed"] == 0, (i, st)
+        assert int(occ[i]) == int((slots != 0).sum()) == len(per_filter[i]), i
+        i1, i2, fp = o.candidates(per_filter[i])
+        assert not orc.check_invariants(slots, o.alt_map(), i1, i2, fp, norm=o.pure_tag), i
+    out = torch.zeros(len(h_keys), dtype=torch.uint8, device="cuda")
+    s.contains_async(d_keys, d_offs, d_filt, out)
+    s.sync()
+    assert host_u8(out).all(), "false negative"
 
 
 @pytest.mark.parametrize("alt,policy,max_ev,fill", [(1, 1, 500, 0.97), (2, 0, 500, 0.97), (2, 1, 16, 1.0)])
@@ -184,14 +272,19 @@ def test_sorted_insert_one_key_per_call_bit_exact(cfb, orc, alt, policy, max_ev,
     assert np.array_equal(image(f), o.table)
 
 
+@pytest.mark.parametrize("staging", [2, 3])
 @pytest.mark.parametrize("alt", [1, 2])
-def test_segment_path_with_partial_last_segment(cfb, orc, alt):
-    """~62 500 buckets: 31 segments of 2048 buckets, the last one partial.
-    Segment-staged inserts, lookups and deletes keep every invariant and agree
-    with the random path on the same image."""
+def test_segment_path_with_partial_last_segment(cfb, orc, alt, staging):
+    """~62 500 buckets: 31 segments of 2048 buckets (segment-staged), or 31
+    regions of 2048 buckets (region-staged, 64 KiB regions), the last one
+    partial.  Staged inserts, lookups and deletes keep every invariant and
+    agree with the random path on the same image."""
     f, o = make(cfb, orc, alt, policy=0, cap=1_000_003)
     assert o.nb % 2048 != 0
-    f.setOption(cfb.OPT_STAGING, 2)  # segment
+    f.setOption(cfb.OPT_STAGING, staging)
+    if staging == 3:
+        f.setOption(cfb.OPT_REGION_BYTES, 1 << 16)
+        assert f.getOption(cfb.OPT_REGION_COUNT) == (o.nb - 1) // 2048 + 1
     keys = orc.splitmix64(31 + alt, int(0.95 * f.capacity()))
     d = dev(keys)
     ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
