@@ -14,7 +14,7 @@
  * Table image: identical to the reference's (CuckooFilter.cuh:224-237): bucket b
  * is bucket_bytes = bucket_size*bits_per_tag/8 contiguous bytes at offset
  * b*bucket_bytes; slot s holds its tag at byte s*bits_per_tag/8 of the bucket,
- * 0 means empty.  num_buckets is a power of two.
+ * 0 means empty.  num_buckets is a power of two under the XOR policy.
  */
 #ifndef CUCKOO_B200_H
 #define CUCKOO_B200_H
@@ -365,6 +365,41 @@ int cf_set_get_launch(const cf_set* s, int op, uint32_t* block, uint32_t* kpt, u
  * leaves it empty.  *best_ms (optional) receives the best trial's time. */
 int cf_set_autotune(cf_set* s, int op, const void* d_keys, uint64_t n, const uint64_t* d_offsets,
                     const uint32_t* d_filters, uint32_t n_items, uint8_t* d_out, void* stream, float* best_ms);
+
+/* ------------------------------------------------------------ key sharding
+ *
+ * The exchange step of the hash-partitioned multi-GPU form (replaces the
+ * reference's Partitioner and gossip multisplit, CuckooFilterMultiGPU.cuh:44-50
+ * and :226-234, and the placement of results, :292-312).  Key k belongs to
+ * shard hash64(k) % num_shards, hash64 being the filter's own 64-bit xxHash of
+ * the key (4- or 8-byte keys).
+ *
+ * Routing CF_SHARD_REFERENCE is the reference's: hash64(k) % num_shards.  With
+ * the XOR policy and a power-of-two shard count it ties the shard to the low
+ * bits of the primary bucket (both come from the low bits of hash64(k)), so a
+ * shard's keys use only 1/num_shards of its buckets as primary buckets (more
+ * evictions, and failed inserts near full load).  CF_SHARD_REMIXED routes by
+ * remix64(hash64(k)) % num_shards instead, remix64 being splitmix64's
+ * bijective output mixer, which keeps shard and buckets independent.
+ *
+ * cf_shard_partition groups a device batch of n keys by shard: d_out_keys
+ * holds shard 0's keys, then shard 1's, and so on; d_out_pos[i] is the batch
+ * position of d_out_keys[i]; d_counts (num_shards uint64 values, device
+ * memory) receives the keys per shard.  The order inside a shard's group is
+ * unspecified.  n < 2^32; num_shards 1..256; d_workspace is device memory of
+ * at least cf_shard_workspace_bytes(n, num_shards) bytes.
+ *
+ * cf_shard_unpartition writes d_out[d_pos[i]] = d_grouped[i] for i < n: per-key
+ * results that come back in group order land at their batch positions.
+ *
+ * Both calls only launch on `stream` (no allocation, no synchronization). */
+typedef enum cf_shard_routing { CF_SHARD_REFERENCE = 0, CF_SHARD_REMIXED = 1 } cf_shard_routing;
+
+uint64_t cf_shard_workspace_bytes(uint64_t n, uint32_t num_shards);
+int cf_shard_partition(const void* d_keys, uint64_t n, uint32_t key_bytes, uint32_t num_shards, uint32_t routing,
+                       void* d_out_keys, uint32_t* d_out_pos, uint64_t* d_counts, void* d_workspace,
+                       uint64_t workspace_bytes, void* stream);
+int cf_shard_unpartition(const uint8_t* d_grouped, const uint32_t* d_pos, uint64_t n, uint8_t* d_out, void* stream);
 
 #ifdef __cplusplus
 }
