@@ -1080,6 +1080,129 @@ def run_policies(args) -> dict:
                                    "keys), 2^28 lookups 50% positive, 2^26 deletes"}, "rows": rows}
 
 
+def run_sharded(args) -> dict | None:
+    """The hash-partitioned multi-GPU form (CuckooFilterMultiGPU: one rank per
+    GPU, keys grouped on the device and exchanged with NCCL all-to-all).  The
+    filter's capacity gives each rank a 2^S-slot shard (16/16, BFS; S =
+    --shard-slots-log2, 28 by default); per rank and step: 0.95 * 2^S keys
+    inserted, 2^(S-1) lookups (half of them the rank's own keys, half never
+    inserted) and 2^(S-2) deletes; CUDA events around each
+    call, max over ranks.  Also the grouping kernels alone on the rank's keys
+    with 8 shards, against their algorithmic bytes (28 B per key for the
+    partition, 6 B for the unpartition)."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    import cuckoo_b200.multigpu as mg
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    own_group = False
+    if not dist.is_initialized():
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", str(port))
+        dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        own_group = True
+    world = dist.get_world_size()
+    peak, peak_src = measured_peak()
+    slots = 1 << args.shard_slots_log2
+    n = int(0.95 * slots)
+    q4 = slots // 4
+    keys = torch.empty(n, dtype=torch.int64, device=dev)
+    splitmix64_torch(11 + 1000 * rank, 0, n, keys)
+    neg = torch.empty(q4, dtype=torch.int64, device=dev)
+    splitmix64_torch(12 + 1000 * rank, 0, q4, neg)
+    query = torch.cat([keys[:q4], neg])
+    dele = keys[q4: 2 * q4].clone()
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    grp = mg.KeyGrouping(dev, 8)
+    holder = {}
+
+    def part():
+        holder["p"] = grp.partition(keys, 8)
+
+    for _ in range(args.warmup):
+        part()
+    part_ms = max_over_ranks(world, timed(part, args.steps))
+    _, pos, _ = holder["p"]
+    res = torch.randint(0, 2, (n,), dtype=torch.uint8, device=dev)
+    unpart_ms = max_over_ranks(world, timed(lambda: grp.unpartition(res, pos), args.steps))
+    del holder, pos, res
+
+    # SDIV(cap, N) * 1.02 stays below `slots`: a `slots`-slot shard per rank
+    cap = int(world * (slots - 64) / 1.02)
+    cfg = cfb.CuckooConfig(T="uint64", bitsPerTag=16, bucketSize=16, evictionPolicy=cfb.EvictionPolicy.BFS,
+                           maxEvictions=500)
+    f = mg.CuckooFilterMultiGPU(cfg, cap, routing=args.routing)
+    assert f.ops.filter.capacity() == slots
+    phases = {"insert": [], "lookup": [], "delete": []}
+    for step in range(args.warmup + args.steps):
+        f.clear()
+        barrier(world)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        f.insertMany(keys)
+        ev[1].record(stream)
+        f.containsMany(query)
+        ev[2].record(stream)
+        f.deleteMany(dele)
+        ev[3].record(stream)
+        torch.cuda.synchronize()
+        if step >= args.warmup:
+            for k, (a, b) in zip(phases, ((0, 1), (1, 2), (2, 3))):
+                phases[k].append(max_over_ranks(world, ev[a].elapsed_time(ev[b])))
+    st = f.ops.filter.stats()
+    failed = int(_reduce(world, float(st["failed"]), "sum"))
+    ms = {k: statistics.median(v) for k, v in phases.items()}
+    step_ms = sum(ms.values())
+    keys_step = world * (n + query.numel() + dele.numel())
+    out = None
+    if rank == 0:
+        out = {"form": "sharded", "metric": "Gkeys/s insert + lookup + delete through CuckooFilterMultiGPU",
+               "value": keys_step / step_ms / 1e6, "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+               "dtype": "u64", "data": "synthetic: splitmix64 keys",
+               "config": {"workload": f"per rank: a 2^{args.shard_slots_log2}-slot shard (16/16, BFS), 0.95 * "
+                                      f"2^{args.shard_slots_log2} inserts, 2^{args.shard_slots_log2 - 1} lookups "
+                                      f"(50% positive), 2^{args.shard_slots_log2 - 2} deletes",
+                          "routing": args.routing},
+               "ops": {k: {"ms": v, "gkeys_s": world * c / v / 1e6}
+                       for (k, v), c in zip(ms.items(), (n, query.numel(), dele.numel()))},
+               "failed_inserts": failed,
+               "grouping": {"shards": 8, "keys": n,
+                            "partition": {"ms": part_ms, "gbs": 28 * n / part_ms / 1e6,
+                                          "frac": 28 * n / part_ms / 1e6 / peak},
+                            "unpartition": {"ms": unpart_ms, "gbs": 6 * n / unpart_ms / 1e6,
+                                            "frac": 6 * n / unpart_ms / 1e6 / peak},
+                            "peak_gbs": peak, "peak_source": peak_src}}
+    if own_group:
+        dist.destroy_process_group()
+    return out
+
+
 # ------------------------------------------------------------ reference arm
 
 
@@ -1187,9 +1310,14 @@ def main() -> None:
     ap.add_argument("--kmer-file", default=None,
                     help="--form kmer: insert the k-mers of this file (u64 count + u64 2-bit k-mers, the "
                          "reference's k-mer benchmark format) instead of synthetic DNA")
-    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid", "policies"), default="plain",
+    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid", "policies", "sharded"),
+                    default="plain",
                     help="batched: the filter-set form over 4096 uneven filters; served: the multi-tenant "
-                         "continuous-batching form (each its own JSON line)")
+                         "continuous-batching form; sharded: the hash-partitioned multi-GPU form (each its own "
+                         "JSON line)")
+    ap.add_argument("--routing", choices=("reference", "remixed"), default="reference",
+                    help="--form sharded: shard routing of CuckooFilterMultiGPU")
+    ap.add_argument("--shard-slots-log2", type=int, default=28, help="--form sharded: log2 slots per rank")
     ap.add_argument("--tenants", type=int, default=256)
     ap.add_argument("--loads", default="10,50,100,200", help="offered loads of the served form, Mkeys/s")
     ap.add_argument("--duration", type=float, default=0.5, help="seconds of arrivals per offered load")
@@ -1210,6 +1338,8 @@ def main() -> None:
         res = run_policies(args)
     elif args.form == "grid":
         res = run_grid(args)
+    elif args.form == "sharded":
+        res = run_sharded(args)
     else:
         res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
     if res is not None:

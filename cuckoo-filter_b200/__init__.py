@@ -148,7 +148,7 @@ def library() -> C.CDLL:
         "cf_get_option": ([vp, i32, P64], i32),
         "cf_shard_workspace_bytes": ([u64, u32], u64),
         "cf_shard_partition": ([vp, u64, u32, u32, u32, vp, vp, vp, vp, u64, vp], i32),
-        "cf_shard_unpartition": ([vp, vp, u64, vp, vp], i32),
+        "cf_shard_unpartition": ([vp, vp, u64, u32, vp, u64, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

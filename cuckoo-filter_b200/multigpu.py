@@ -47,13 +47,17 @@ def capacity_per_gpu(capacity: int, num_gpus: int) -> int:
 
 class KeyGrouping:
     """The grouping kernels (``cf_shard_partition`` / ``cf_shard_unpartition``)
-    on one device, with their workspace."""
+    on one device, with their workspace.  ``unpartition`` reads the run starts
+    that the last ``partition`` left in the workspace, so it takes the results
+    of that batch."""
 
     def __init__(self, device, key_bytes: int):
         import torch
 
         self.torch, self.device, self.key_bytes = torch, torch.device(device), int(key_bytes)
         self._ws = None
+        self._wsb = 0
+        self._ns = 0
         self._L = library()
 
     def partition(self, keys, num_shards: int, routing: int = 0):
@@ -73,14 +77,19 @@ class KeyGrouping:
         _check(self._L.cf_shard_partition(keys.data_ptr() or None, n, self.key_bytes, num_shards, int(routing),
                                           grouped.data_ptr() or None, pos.data_ptr() or None, counts.data_ptr(),
                                           self._ws.data_ptr(), wsb, _stream_handle(None)))
+        self._wsb, self._ns = wsb, num_shards
         return grouped, pos, counts
 
     def unpartition(self, grouped, pos):
-        """Per-key bytes in group order back at their batch positions."""
+        """Per-key bytes of the last partitioned batch, in group order, back
+        at their batch positions."""
         n = grouped.numel()
+        if self._ns == 0:
+            raise RuntimeError("unpartition before any partition")
         out = self.torch.empty(n, dtype=self.torch.uint8, device=self.device)
-        _check(self._L.cf_shard_unpartition(grouped.data_ptr() or None, pos.data_ptr() or None, n,
-                                            out.data_ptr() or None, _stream_handle(None)))
+        _check(self._L.cf_shard_unpartition(grouped.data_ptr() or None, pos.data_ptr() or None, n, self._ns,
+                                            self._ws.data_ptr(), self._wsb, out.data_ptr() or None,
+                                            _stream_handle(None)))
         return out
 
 

@@ -390,7 +390,10 @@ int cf_set_autotune(cf_set* s, int op, const void* d_keys, uint64_t n, const uin
  * at least cf_shard_workspace_bytes(n, num_shards) bytes.
  *
  * cf_shard_unpartition writes d_out[d_pos[i]] = d_grouped[i] for i < n: per-key
- * results that come back in group order land at their batch positions.
+ * results that come back in group order land at their batch positions.  It
+ * reads the run starts that cf_shard_partition of the same batch (same n and
+ * num_shards) left in d_workspace, so the workspace must be untouched in
+ * between; otherwise the results are undefined (no access leaves the arrays).
  *
  * Both calls only launch on `stream` (no allocation, no synchronization). */
 typedef enum cf_shard_routing { CF_SHARD_REFERENCE = 0, CF_SHARD_REMIXED = 1 } cf_shard_routing;
@@ -399,7 +402,8 @@ uint64_t cf_shard_workspace_bytes(uint64_t n, uint32_t num_shards);
 int cf_shard_partition(const void* d_keys, uint64_t n, uint32_t key_bytes, uint32_t num_shards, uint32_t routing,
                        void* d_out_keys, uint32_t* d_out_pos, uint64_t* d_counts, void* d_workspace,
                        uint64_t workspace_bytes, void* stream);
-int cf_shard_unpartition(const uint8_t* d_grouped, const uint32_t* d_pos, uint64_t n, uint8_t* d_out, void* stream);
+int cf_shard_unpartition(const uint8_t* d_grouped, const uint32_t* d_pos, uint64_t n, uint32_t num_shards,
+                         const void* d_workspace, uint64_t workspace_bytes, uint8_t* d_out, void* stream);
 
 #ifdef __cplusplus
 }

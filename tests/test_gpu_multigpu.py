@@ -89,7 +89,7 @@ def test_emulated_shards_on_one_gpu(cfb, orc, ns, routing):
     owner = mg.shard_of(keys, ns, routing=rname)
     q = np.concatenate([keys[::5], orc.splitmix64(99, 300_000)])
     qo = mg.shard_of(q, ns, routing=rname)
-    ops2, gq, posq, cq = partition(mg, dev(q), ns, 8, routing)
+    ops2, gq, posq, cq = partition(mg, dev(q), ns, 8, routing)  # ops2 keeps q's run starts
     cqs = np.concatenate([[0], np.cumsum(cq.cpu().numpy())]).astype(np.int64)
     res = torch.empty(len(q), dtype=torch.uint8, device="cuda")
     for s in range(ns):
