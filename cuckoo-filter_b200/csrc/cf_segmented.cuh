@@ -487,12 +487,15 @@ enum SegOp : int { SEG_INSERT = 0, SEG_CONTAINS = 1, SEG_DELETE = 2 };
 // misses are appended (keyed by the alternate bucket) to `next`.  round 2:
 // entries carry the alternate bucket; insert misses are appended to `next`
 // for eviction, lookup/delete misses are final.  Hits set bit `payload` of
-// `bitmap` when a bitmap is given.
+// `bitmap` when a bitmap is given.  fwd_other: forwarded entries are keyed by
+// the key's other bucket (set in round 1).  `cap` is used by k_seg_insert
+// only (the two kernels share a launch site).
 template <class C, int OP>
 __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                      const uint32_t* start, uint64_t nseg, int sb_log2, int round,
                                                      uint64_t* next, uint32_t* next_pay,
-                                                     unsigned long long* next_count, uint32_t* bitmap, int narrow) {
+                                                     unsigned long long* next_count, uint32_t* bitmap, int narrow,
+                                                     uint32_t /*cap*/, int fwd_other) {
     extern __shared__ __align__(16) uint64_t seg[];
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_base;
@@ -591,7 +594,7 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
                       // the full bucket index from the segment (entries may be 4-byte)
                       uint64_t b = (s << sb_log2) | ((e >> C::bits) & (sb - 1));
                       uint32_t tg = fp;
-                      if (round == 1) {  // keyed by the alternate bucket, the tag in that bucket's form
+                      if (fwd_other) {  // keyed by the other bucket, the tag in that bucket's form
                           b = alt_bucket<C>(b, fp, t.nb_mask);
                           tg = alt_tag<C>(fp);
                       }
@@ -616,7 +619,7 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
         __syncthreads();
     }
     if constexpr (OP == SEG_INSERT) {
-        flush_counter(&t.ctr[round == 1 ? CTR_PRIMARY : CTR_SECONDARY], n_ok);
+        flush_counter(&t.ctr[round == 2 ? CTR_SECONDARY : CTR_PRIMARY], n_ok);
         flush_counter(&t.ctr[CTR_OCCUPIED], n_ok);
     } else if constexpr (OP == SEG_DELETE) {
         const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, n_ok);
@@ -875,6 +878,14 @@ constexpr size_t seg_insert_smem(int sb_log2) {
     return (static_cast<size_t>(1) << sb_log2) * (C::bucket_bytes + sizeof(SlotMask<C>));
 }
 
+template <class M>
+__device__ __forceinline__ uint32_t popc_mask(M m) {
+    if constexpr (sizeof(M) == 8)
+        return static_cast<uint32_t>(__popcll(static_cast<unsigned long long>(m)));
+    else
+        return static_cast<uint32_t>(__popc(static_cast<unsigned int>(m)));
+}
+
 // Empty-slot mask of a bucket image (bit s set when slot s holds 0).
 template <class C>
 __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
@@ -905,8 +916,12 @@ __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
 // reference's tryInsertAtBucket scans words and lanes (CuckooFilter.cuh:859-904)
 // -- claimed with one atomic AND on the mask, then written into the slot
 // with a plain store (the claim makes the slot the thread's own).  Tags whose
-// bucket is full go to `next`: keyed by the alternate bucket in round 1,
-// unchanged (for eviction) in round 2.
+// bucket is full go to `next`, keyed by the key's other bucket when
+// fwd_other is set, else unchanged (for eviction).
+// cap: a claim succeeds only while the bucket holds fewer than `cap` tags
+// (C::bs: no limit).  A claim that finds `cap` tags already there gives its
+// slot back, so at most `cap` claims succeed per bucket; a racing claim may
+// see the returned slot as taken and forward its tag, which is always allowed.
 // PAY: entries carry payloads (key positions; `pay`, `next_pay` and `bitmap`
 // are used only then).
 template <class C, bool PAY>
@@ -914,7 +929,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                                                             const uint32_t* start, uint64_t nseg, int sb_log2,
                                                             int round, uint64_t* next, uint32_t* next_pay,
                                                             unsigned long long* next_count, uint32_t* bitmap,
-                                                            int narrow) {
+                                                            int narrow, uint32_t cap, int fwd_other) {
     using M = SlotMask<C>;
     extern __shared__ __align__(16) uint64_t seg[];
     __shared__ uint32_t s_warp[32];
@@ -983,6 +998,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                 M m = mask[lb];
                 bool ok = false;
                 for (int it = 0; it < 64 && m; ++it) {
+                    if (C::bs - popc_mask(m) >= cap) break;  // `cap` tags there already
                     // first empty slot circularly from s0
                     const M rot = s0 ? (((m >> s0) | (m << (C::bs - s0))) & kFull) : m;
                     uint32_t off;
@@ -994,6 +1010,10 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                     // claim the slot alone: only a claim of the same slot can fail
                     const M bit = static_cast<M>(1) << slot;
                     const M old = atomicAnd(&mask[lb], ~bit);
+                    if ((old & bit) && C::bs - popc_mask(old) >= cap) {  // claimed past the cap: give it back
+                        atomicOr(&mask[lb], bit);
+                        break;
+                    }
                     if (old & bit) {
                         uint8_t* dst = seg_bytes + (static_cast<uint64_t>(lb) * C::bucket_bytes + slot * TB);
                         if constexpr (TB == 1)
@@ -1035,7 +1055,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                         // the full bucket index from the segment (entries may be 4-byte)
                         uint64_t b = (s << sb_log2) | ((ev[j] >> C::bits) & (sb - 1));
                         uint32_t tg = fp;
-                        if (round == 1) {  // keyed by the alternate bucket, the tag in that bucket's form
+                        if (fwd_other) {  // keyed by the other bucket, the tag in that bucket's form
                             b = alt_bucket<C>(b, fp, t.nb_mask);
                             tg = alt_tag<C>(fp);
                         }
@@ -1056,7 +1076,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
         }
         __syncthreads();
     }
-    flush_counter(&t.ctr[round == 1 ? CTR_PRIMARY : CTR_SECONDARY], n_ok);
+    flush_counter(&t.ctr[round == 2 ? CTR_SECONDARY : CTR_PRIMARY], n_ok);
     flush_counter(&t.ctr[CTR_OCCUPIED], n_ok);
 }
 
