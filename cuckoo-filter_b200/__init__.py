@@ -53,6 +53,7 @@ OPT_REGION_COUNT = 8
 OPT_LOOKUP_KPT = 9
 OPT_PERSISTENT = 10
 OPT_CHAIN_HISTOGRAM = 11
+OPT_ROUND1_CAP = 12
 NEVER = (1 << 64) - 1
 
 # cf_staging values (OPT_STAGING)

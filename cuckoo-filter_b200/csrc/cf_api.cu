@@ -42,6 +42,7 @@ struct cf_filter {
     uint64_t ws_limit;      // CF_OPT_WORKSPACE_LIMIT
     uint64_t seg_min_keys;  // CF_OPT_SEGMENTED_MIN_KEYS (0 = automatic)
     uint64_t round2_min;    // CF_OPT_ROUND2_SEGMENTED_MIN_KEYS (0 = automatic)
+    uint32_t round1_cap;    // CF_OPT_ROUND1_CAP (0 = automatic)
     unsigned long long* h_cnt;
     // region-staged path
     RegionGeom rgeom;
@@ -322,6 +323,7 @@ int run_segmented(cf_filter* f, int op, const void* keys, uint64_t n, uint8_t* o
     SegWork w{};
     if (int st = ensure_workspace(f, n, out != nullptr, &w)) return st;
     w.round2_segmented_min = f->round2_min ? f->round2_min : auto_threshold(f, op);
+    w.round1_cap = f->round1_cap;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint64_t kb = f->cfg.key_bytes;
     for (uint64_t c0 = 0; c0 < n; c0 += w.cap) {
@@ -734,6 +736,11 @@ int cf_set_option(cf_filter* f, int option, uint64_t value) {
             if (value > 1) return fail(CF_ERR_INVALID, "chain histogram must be 0 or 1");
             f->chain_hist = static_cast<uint32_t>(value);
             return CF_OK;
+        case CF_OPT_ROUND1_CAP:
+            if (value > f->cfg.bucket_size)
+                return fail(CF_ERR_INVALID, "round-1 cap must be 0 (automatic) or 1..bucket_size");
+            f->round1_cap = static_cast<uint32_t>(value);
+            return CF_OK;
         case CF_OPT_REGION_BYTES:
             if (value & (value - 1)) return fail(CF_ERR_INVALID, "region bytes must be 0 or a power of two");
             f->rg_bytes = value;
@@ -758,6 +765,7 @@ int cf_get_option(cf_filter* f, int option, uint64_t* value) {
         case CF_OPT_REGION_COUNT: *value = f->rgeom.nreg; return CF_OK;
         case CF_OPT_LOOKUP_KPT: *value = f->lookup_kpt; return CF_OK;
         case CF_OPT_PERSISTENT: *value = f->persistent; return CF_OK;
+        case CF_OPT_ROUND1_CAP: *value = f->round1_cap; return CF_OK;
         case CF_OPT_CHAIN_HISTOGRAM: *value = f->chain_hist; return CF_OK;
         default: return fail(CF_ERR_INVALID, "unknown option %d", option);
     }
@@ -960,6 +968,7 @@ int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8
     w.sms = f->sms;
     w.rg_grid = f->sms * 4;
     w.round2_segmented_min = f->round2_min ? f->round2_min : auto_threshold(f, SEG_INSERT);
+    w.round1_cap = f->round1_cap;
     if (n) {
         // the segment pass clears the list counters, the result bitmap and the
         // segment starts itself; the other buffers are written before read

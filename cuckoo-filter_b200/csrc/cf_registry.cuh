@@ -47,6 +47,7 @@ struct SegWork {
     int rs_grid[3];  // radix CTAs per payload mode (one wave of that scatter kernel)
     int sms;       // streaming multiprocessors
     uint64_t round2_segmented_min;  // list length from which round 2 is segment-staged
+    uint32_t round1_cap;            // CF_OPT_ROUND1_CAP (0 = automatic)
     int rg_grid;   // CTAs of the region partition kernels (hist entries: kRgMaxRegions * rg_grid)
 };
 
@@ -362,7 +363,10 @@ struct Launchers {
         // third round, and only what misses that goes to eviction.  Far
         // fewer keys need eviction: 4.0 % of a 0.95 fill of 16-slot buckets
         // after two uncapped rounds, 2.0 % after the three capped ones.
-        const uint32_t cap1 = OP == SEG_INSERT && C::bs <= 64 && m >= t.nb_mask + 1 ? round1_cap() : C::bs;
+        const uint32_t cap1 = OP != SEG_INSERT || C::bs > 64 ? C::bs
+                              : w.round1_cap                 ? w.round1_cap
+                              : m >= t.nb_mask + 1           ? round1_cap()
+                                                             : C::bs;
         const bool round3 = cap1 < C::bs;
         if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a, &have_start, &narrow);
         if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, narrow, s, cap1, 1);

@@ -226,7 +226,15 @@ typedef enum cf_option {
     /* 1 = record the eviction-chain-length histogram of inserts
      * (cf_get_chain_histogram); 0 = off (default; one atomic per evicting
      * insert when on). */
-    CF_OPT_CHAIN_HISTOGRAM = 11
+    CF_OPT_CHAIN_HISTOGRAM = 11,
+    /* Segment-staged inserts of at least one key per bucket: tags the first
+     * round (primary buckets) may leave in a bucket.  0 = automatic: 13 of
+     * 16 slots (bucket_size minus 3/16 of it), the keys that miss their
+     * primary and then their alternate bucket get a third round at the
+     * primary bucket before eviction; bucket_size = no limit and no third
+     * round (the reference's primary-first order: a key goes to its
+     * alternate bucket only when its primary is full).  1..bucket_size. */
+    CF_OPT_ROUND1_CAP = 12
 } cf_option;
 
 /* Eviction-chain-length histogram since creation, cf_clear or cf_reset_stats,

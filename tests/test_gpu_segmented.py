@@ -248,3 +248,35 @@ def test_insertMany_stages_batches_of_at_least_one_key_per_bucket(cfb, orc):
     c3 = cfb.launch_count()
     f.insertMany(dev(big))
     assert cfb.launch_count() - c3 <= 2
+
+
+def test_round1_cap_option(cfb, orc):
+    """CF_OPT_ROUND1_CAP on a 0.95 sorted fill: automatic (13 of 16 slots in
+    the first round, a third round at the primary bucket), the reference's
+    primary-first order (16) and an explicit 12 all keep every invariant; the
+    automatic cap sends more keys to their alternate bucket and leaves fewer
+    for eviction than the primary-first order."""
+    res = {}
+    for capv in (0, 16, 12):
+        f, o = make(cfb, orc, 8, 16, 16, 1, 500, 1 << 20)
+        f.setOption(cfb.OPT_ROUND1_CAP, capv)
+        assert f.getOption(cfb.OPT_ROUND1_CAP) == capv
+        keys = orc.splitmix64(77, int(0.95 * f.capacity()))
+        d = dev(keys)
+        ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
+        occ = f.insertManySorted(d, d_output=ok_t)
+        st = f.stats()
+        ok = host_u8(ok_t).astype(bool)
+        assert occ == ok.sum() == f.countOccupiedSlots() and st["lost"] == 0, (capv, st)
+        assert st["primary"] + st["secondary"] + st["evicted_inserts"] == len(keys)
+        assert host_u8(f.containsMany(d[ok_t])).all(), "false negative"
+        errs = _stored_invariants(f, o, orc, keys[ok])
+        assert not errs, (capv, errs)
+        res[capv] = st
+        f.close()
+    assert res[0]["secondary"] > res[16]["secondary"]
+    assert res[0]["evicted_inserts"] < res[16]["evicted_inserts"], (res[0], res[16])
+    f, _ = make(cfb, orc, 8, 16, 16, 1, 500, 1 << 12)
+    with pytest.raises(cfb.CuckooError):
+        f.setOption(cfb.OPT_ROUND1_CAP, 17)
+    f.close()
