@@ -70,7 +70,7 @@ def test_golden_fp_zero_maps_to_one(golden):
     assert found > 0
 
 
-def test_known_answers_from_survey(orc):
+def test_known_answers_for_keys_1_and_42(orc):
     """Known answers computed from the reference headers for key 1 and key 42
     at 16-bit tags, bucket size 16, 2^16 buckets."""
     f = orc.OracleFilter(capacity=1 << 20)
