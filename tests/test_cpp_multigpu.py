@@ -46,3 +46,42 @@ def test_multigpu_header_on_one_gpu(cfb):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "0 failures" in r.stdout and r.stdout.count("[  OK  ]") == 5, r.stdout
+
+
+HOST_PROGRAM = r"""
+#include <CuckooFilterMultiGPU.cuh>
+#include <cstdio>
+#include <vector>
+using C = CuckooConfig<uint64_t, 16, 500, 256, 16, XorAltBucketPolicy, EvictionPolicy::BFS>;
+int main(int argc, char**) {
+    if (argc > 5) {  // every member instantiated; nothing runs without a GPU
+        CuckooFilterMultiGPU<C> f(2, 1 << 20);
+        std::vector<uint64_t> k(10);
+        std::vector<bool> o;
+        f.insertMany(k);
+        f.containsMany(k, o);
+        f.deleteMany(k, o);
+        f.deleteMany(k);
+        std::printf("%f %zu %zu %zu\n", f.loadFactor(), f.totalOccupiedSlots(), f.totalCapacity(), f.sizeInBytes());
+        f.clear();
+        f.synchronizeAllGPUs();
+    }
+    std::printf("0\n");
+    return 0;
+}
+"""
+
+
+def test_multigpu_header_compiles_with_host_compiler(cfb, tmp_path):
+    cuda = "/usr/local/cuda"
+    if not shutil.which("g++") or not os.path.isdir(os.path.join(cuda, "include")):
+        pytest.skip("g++ or the CUDA headers are missing")
+    src = tmp_path / "host.cpp"
+    src.write_text(HOST_PROGRAM)
+    exe = tmp_path / "host"
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", f"-I{INC}", f"-I{cuda}/include", str(src),
+                        f"-L{LIBDIR}", "-lcuckoo_b200", f"-Wl,-rpath,{LIBDIR}", f"-L{cuda}/lib64", "-lcudart",
+                        f"-Wl,-rpath,{cuda}/lib64", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0 and run.stdout.strip() == "0", run.stdout + run.stderr
