@@ -98,6 +98,124 @@ def splitmix64_torch(seed: int, first: int, n: int, out, chunk: int = 1 << 27):
     return out
 
 
+# ------------------------------------------- parity check: hashing and digests
+#
+# An independent restatement, in torch int64 arithmetic, of the reference's
+# key hashing (xxHash64 with seed 0 over the value's little-endian bytes,
+# reference include/hashutil.cuh:71-161) and of XorAltBucketPolicy
+# (bucket_policies.cuh:46-74).  It shares no code with the library's kernels,
+# so it can check a table the kernels built; tests pin it to the golden vectors
+# made from the reference's own headers.  int64 products wrap modulo 2^64.
+
+XXH_P1, XXH_P2, XXH_P3 = 0x9E3779B185EBCA87, 0xC2B2AE3D27D4EB4F, 0x165667B19E3779F9
+XXH_P4, XXH_P5 = 0x85EBCA77C2B2AE63, 0x27D4EB2F165667C5
+
+
+def _lsr(z, s: int):
+    return (z >> s) & ((1 << (64 - s)) - 1)
+
+
+def _rotl(z, r: int):
+    return (z << r) | _lsr(z, 64 - r)
+
+
+def _xxh_avalanche(h):
+    h = (h ^ _lsr(h, 33)) * s64(XXH_P2)
+    h = (h ^ _lsr(h, 29)) * s64(XXH_P3)
+    return h ^ _lsr(h, 32)
+
+
+def xxh64_torch(v, nbytes: int):
+    """XXH64 (seed 0) of each value of the int64 tensor `v`, read as `nbytes`
+    (1, 2, 4 or 8) little-endian bytes."""
+    h = v * 0 + s64(XXH_P5 + nbytes)
+    if nbytes == 8:
+        k1 = _rotl(v * s64(XXH_P2), 31) * s64(XXH_P1)
+        h = _rotl(h ^ k1, 27) * s64(XXH_P1) + s64(XXH_P4)
+    elif nbytes == 4:
+        h = _rotl(h ^ ((v & 0xFFFFFFFF) * s64(XXH_P1)), 23) * s64(XXH_P2) + s64(XXH_P3)
+    else:
+        for i in range(nbytes):
+            h = _rotl(h ^ (((v >> (8 * i)) & 0xFF) * s64(XXH_P5)), 11) * s64(XXH_P1)
+    return _xxh_avalanche(h)
+
+
+def tag_hash_table(bits: int, device):
+    """xxHash64 of every tag value of a bits-bit TagType (8 or 16 bits) as a lookup table."""
+    import torch
+
+    return xxh64_torch(torch.arange(1 << bits, dtype=torch.int64, device=device), bits // 8)
+
+
+def candidates_torch(keys, key_bytes: int, bits: int, num_buckets: int, tag_lut=None):
+    """(i1, i2, fp) of XorAltBucketPolicy::getCandidateBuckets: fp from the
+    upper 32 hash bits masked to `bits` (0 becomes 1), i1 from the lower 32 bits
+    masked to the bucket count, i2 = i1 ^ (xxHash64(fp as TagType) & (nB - 1))."""
+    h = xxh64_torch(keys if key_bytes == 8 else keys & 0xFFFFFFFF, key_bytes)
+    fp = _lsr(h, 32) & ((1 << bits) - 1)
+    fp = fp + (fp == 0).to(fp.dtype)
+    mask = num_buckets - 1
+    i1 = h & 0xFFFFFFFF & mask
+    th = tag_lut[fp] if tag_lut is not None else xxh64_torch(fp, bits // 8)
+    return i1, i1 ^ (th & mask), fp
+
+
+_DIGEST_SEEDS = (0x2545F4914F6CDD1D, 0x7FB5D329728EA185)
+
+
+def _digest_add(acc: list, sig, valid) -> None:
+    """acc += (count, sum of two 32-bit mixes) over sig[valid], exactly (Python ints)."""
+    import torch
+
+    sig = sig[valid]
+    acc[0] += int(sig.numel())
+    for j, seed in enumerate(_DIGEST_SEEDS):
+        z = sig + s64(seed)
+        z = (z ^ _lsr(z, 30)) * s64(M1)
+        z = (z ^ _lsr(z, 27)) * s64(M2)
+        acc[1 + j] += int(_lsr(z ^ _lsr(z, 31), 32).sum(dtype=torch.int64).item())
+
+
+def key_digest(keys, bits: int, num_buckets: int, valid=None, chunk: int = 1 << 26) -> tuple:
+    """Multiset digest of the (bucket pair, tag) entries that storing `keys`
+    (int64 tensor of 8-byte keys; rows with valid == False skipped) must leave in
+    the table: per key, (min(i1, i2) << bits) | fp, mixed and summed."""
+    import torch
+
+    lut = tag_hash_table(bits, keys.device) if bits <= 16 else None
+    acc = [0, 0, 0]
+    for a in range(0, keys.numel(), chunk):
+        k = keys[a:a + chunk]
+        i1, i2, fp = candidates_torch(k, 8, bits, num_buckets, lut)
+        v = valid[a:a + chunk] if valid is not None else torch.ones_like(fp, dtype=torch.bool)
+        _digest_add(acc, (torch.minimum(i1, i2) << bits) | fp, v)
+    return tuple(acc)
+
+
+def table_digest(table_u8, bits: int, bucket_size: int, num_buckets: int, chunk_slots: int = 1 << 26) -> tuple:
+    """Multiset digest of the table image (uint8 tensor, the reference's layout):
+    for every occupied slot of bucket b holding tag t, (min(b, alt(b, t)) << bits) | t."""
+    import torch
+
+    view = {8: torch.uint8, 16: torch.int16, 32: torch.int32}[bits]
+    slots = table_u8.view(view)
+    lut = tag_hash_table(bits, slots.device) if bits <= 16 else None
+    mask = num_buckets - 1
+    acc = [0, 0, 0]
+    per = chunk_slots // bucket_size * bucket_size
+    for a in range(0, slots.numel(), per):
+        t = slots[a:a + per].to(torch.int64) & ((1 << bits) - 1)
+        b = (torch.arange(t.numel(), device=t.device, dtype=torch.int64) + a) // bucket_size
+        th = lut[t] if lut is not None else xxh64_torch(t, 4)
+        _digest_add(acc, (torch.minimum(b, b ^ (th & mask)) << bits) | t, t != 0)
+    return tuple(acc)
+
+
+def digest_sub(a: tuple, b: tuple) -> tuple:
+    """Digest of multiset a minus multiset b (b contained in a)."""
+    return tuple(x - y for x, y in zip(a, b))
+
+
 def negative_collisions(seed_pos: int, n_pos: int, seed_neg: int, n_neg: int) -> list[int]:
     """Indices j of splitmix64(seed_neg) outputs equal to some splitmix64(seed_pos)
     output with index < n_pos.  splitmix64 is a bijection of its state, so
@@ -119,8 +237,10 @@ def collides(seed_pos: int, n_pos: int, seed_neg: int, j: int) -> bool:
     return (j + c) % U64 < n_pos
 
 
-def make_inputs(w: dict, device, rank: int = 0):
-    """Device tensors: fill keys, query keys (positives and negatives shuffled), delete keys."""
+def make_inputs(w: dict, device, rank: int = 0, with_mask: bool = False):
+    """Device tensors: fill keys, query keys (positives and negatives shuffled),
+    delete keys, the number of negatives replaced; with `with_mask` also a bool
+    tensor marking the positives of the query batch."""
     import torch
 
     seed_fill = w["seed_fill"] + 1000 * rank
@@ -155,8 +275,11 @@ def make_inputs(w: dict, device, rank: int = 0):
     g = torch.Generator(device=device)
     g.manual_seed(w["seed_sample"] + 17 + rank)
     query = torch.cat([pos, neg])
-    query = query[torch.randperm(query.numel(), generator=g, device=device)]
+    perm = torch.randperm(query.numel(), generator=g, device=device)
+    query = query[perm]
     dele = pos[: w["n_del"]].clone()
+    if with_mask:
+        return fill, query, dele, len(bad), perm < n_pos
     return fill, query, dele, len(bad)
 
 
@@ -304,38 +427,114 @@ def aggregate(world, keys_per_step: int, steps: int, total_ms: float) -> tuple[f
 # ------------------------------------------------------------ CPU baselines
 
 
-def cpu_sample(scale_log2: int, threads: int, seed: int = 3) -> dict:
-    """The oracle's multithreaded port of the reference algorithm on the host:
-    a 2^scale_log2-slot filter (16/16, BFS) filled to 0.95, lookups of 2^(s-3)
-    keys (50 % positive), deletes of 2^(s-5) stored keys."""
-    import ctypes as C
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
 
-    import numpy as np
+    return platform.processor() or "unknown"
 
-    import oracle
 
-    cap = 1 << scale_log2
-    f = oracle.OracleFilter(key_bytes=8, bits=16, bucket_size=16, policy=oracle.POLICY_BFS, capacity=cap)
-    n_fill = int(0.95 * cap)
-    keys = oracle.splitmix64(seed, n_fill)
-    nq = 1 << (scale_log2 - 3)
-    q = np.concatenate([keys[: nq // 2], oracle.splitmix64(seed + 1, nq // 2)])
-    nd = 1 << (scale_log2 - 5)
-    out = np.empty(max(n_fill, nq), np.uint8)
-    L = oracle.lib()
-    t0 = time.perf_counter()
-    L.cfo_insert_mt(C.byref(f.p), f.table.ctypes.data, keys.ctypes.data, n_fill, None, threads)
-    t1 = time.perf_counter()
-    L.cfo_contains_mt(C.byref(f.p), f.table.ctypes.data, q.ctypes.data, nq, out.ctypes.data, threads)
-    t2 = time.perf_counter()
-    L.cfo_delete_mt(C.byref(f.p), f.table.ctypes.data, keys.ctypes.data, nd, None, threads)
-    t3 = time.perf_counter()
-    total = n_fill + nq + nd
-    return {"value": total / (t3 - t0) / 1e9, "unit": "Gkeys/s", "cores": threads, "kind": "port",
-            "sample": f"2^{scale_log2}-slot 16/16 BFS filter filled to 0.95 ({n_fill} keys), {nq} lookups "
-                      f"(50% positive), {nd} deletes; oracle/cf_oracle.c multithreaded port",
-            "insert_gkeys_s": n_fill / (t1 - t0) / 1e9, "contains_gkeys_s": nq / (t2 - t1) / 1e9,
-            "delete_gkeys_s": nd / (t3 - t2) / 1e9, "seconds": t3 - t0}
+class CpuFullTable:
+    """The reference's algorithm on the host cores (the oracle's port of
+    CuckooFilter.cuh:805-1116 with atomic compare-and-swap on 64-bit words,
+    oracle/cf_oracle.c) on the workload's full-size table.
+
+    fill(): the whole fill once, in 20 load strata; in each stratum the first
+    1/64 of its keys is inserted by one thread and the rest by all threads, so
+    both rates are averaged over the same 0 -> 0.95 load range.
+    step(k): on the full table at 0.95 load, slice k of the lookup batch and of
+    the delete batch by all threads and a 1/16 sub-slice by one thread (deleted
+    keys are re-inserted, untimed, so every step sees the same table).
+    Rates combine as the workload's own mix: (fill + lookups + deletes) keys
+    over fill / r_insert + lookups / r_lookup + deletes / r_delete."""
+
+    STRATA, ONE_IN = 20, 64
+
+    def __init__(self, w: dict, fill, query, dele, threads: int, q_slice: int = 1 << 22, d_slice: int = 1 << 20):
+        import oracle
+
+        self.oracle = oracle
+        self.L = oracle.lib()
+        pol = oracle.POLICY_BFS if w["policy"] == "BFS" else oracle.POLICY_DFS
+        self.o = oracle.OracleFilter(key_bytes=8, bits=w["bits"], bucket_size=w["bs"], policy=pol,
+                                     max_evictions=w["max_ev"], capacity=w["capacity"])
+        self.fill_keys, self.query, self.dele = fill, query, dele
+        self.threads = threads
+        self.q_slice, self.d_slice = min(q_slice, len(query)), min(d_slice, len(dele))
+        self.n = (len(fill), len(query), len(dele))
+        self.rates = {}
+
+    def _run(self, fn, keys, a: int, m: int, threads: int) -> float:
+        import ctypes as C
+
+        t0 = time.perf_counter()
+        fn(C.byref(self.o.p), self.o.table.ctypes.data, keys.ctypes.data + 8 * a, m, None, threads)
+        return time.perf_counter() - t0
+
+    def fill(self) -> None:
+        n = len(self.fill_keys)
+        t1 = tn = 0.0
+        n1 = nn = 0
+        for k in range(self.STRATA):
+            a, b = k * n // self.STRATA, (k + 1) * n // self.STRATA
+            s = max(1, (b - a) // self.ONE_IN)
+            t1 += self._run(self.L.cfo_insert_mt, self.fill_keys, a, s, 1)
+            tn += self._run(self.L.cfo_insert_mt, self.fill_keys, a + s, b - a - s, self.threads)
+            n1 += s
+            nn += b - a - s
+        self.rates["insert"] = {1: n1 / t1, self.threads: nn / tn}
+        self.fill_seconds = t1 + tn
+        self.load = self.o.occupied() / float(self.o.nb * self.o.bucket_size)
+
+    def step(self, k: int) -> dict:
+        nq, nd = len(self.query), len(self.dele)
+        qa = (k * self.q_slice) % max(1, nq - self.q_slice + 1)
+        da = (k * self.d_slice) % max(1, nd - self.d_slice + 1)
+        q1, d1 = max(1, self.q_slice // 16), max(1, self.d_slice // 16)
+        r = {"contains": {}, "delete": {}}
+        L = self.L
+        r["contains"][self.threads] = self.q_slice / self._run(L.cfo_contains_mt, self.query, qa, self.q_slice,
+                                                               self.threads)
+        r["contains"][1] = q1 / self._run(L.cfo_contains_mt, self.query, qa, q1, 1)
+        r["delete"][self.threads] = self.d_slice / self._run(L.cfo_delete_mt, self.dele, da, self.d_slice,
+                                                             self.threads)
+        self._run(L.cfo_insert_mt, self.dele, da, self.d_slice, self.threads)
+        r["delete"][1] = d1 / self._run(L.cfo_delete_mt, self.dele, da, d1, 1)
+        self._run(L.cfo_insert_mt, self.dele, da, d1, self.threads)
+        out = {}
+        for t in (1, self.threads):
+            secs = (self.n[0] / self.rates["insert"][t] + self.n[1] / r["contains"][t]
+                    + self.n[2] / r["delete"][t])
+            out[t] = {"value": sum(self.n) / secs / 1e9, "seconds_per_step": secs,
+                      "insert_gkeys_s": self.rates["insert"][t] / 1e9,
+                      "contains_gkeys_s": r["contains"][t] / 1e9, "delete_gkeys_s": r["delete"][t] / 1e9}
+        return out
+
+    def describe(self) -> str:
+        return (f"full-size {self.o.nb * self.o.bucket_size}-slot table (oracle/cf_oracle.c port of the reference "
+                f"algorithm): one fill of all {self.n[0]} keys in {self.STRATA} load strata (1/{self.ONE_IN} of each "
+                f"stratum by one thread, the rest by {self.threads}), reaching load {self.load:.4f}; per step at that "
+                f"load, {self.q_slice} lookups and {self.d_slice} deletes by {self.threads} threads and 1/16 of each "
+                f"by one thread; the step's rate is the workload's mix ({self.n[0]} inserts, {self.n[1]} lookups, "
+                f"{self.n[2]} deletes) at the measured per-op rates")
+
+
+def cpu_baseline_entry(tab: "CpuFullTable", per_step: list) -> dict:
+    """cpu_baseline object: the all-threads figure as `value`, and both thread counts."""
+    th = tab.threads
+    entries = {}
+    for t in (1, th):
+        v = [s[t] for s in per_step]
+        entries[f"threads_{t}"] = {k: statistics.mean(x[k] for x in v) for k in v[0]}
+    return {"value": entries[f"threads_{th}"]["value"], "unit": "Gkeys/s", "cores": th, "kind": "port",
+            "sample": tab.describe(), "cpu_model": cpu_model(), "fill_seconds": tab.fill_seconds,
+            "threads": {"1": entries["threads_1"], str(th): entries[f"threads_{th}"]}}
 
 
 def host_threads() -> int:
@@ -343,6 +542,25 @@ def host_threads() -> int:
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+def workload_config(args, w: dict, world: int) -> dict:
+    """The `config` object of the plain form's JSON line: the workload alone,
+    identical in the library's arm and the reference arm."""
+    import oracle
+
+    cap, bs, bits = w["capacity"], w["bs"], w["bits"]
+    nb = oracle.num_buckets(cap, bs)
+    n_fill = int(w["fill"] * cap)
+    sorted_fill = args.insert == "sorted" or (args.insert == "auto" and n_fill >= (1 << 29))
+    return {"workload": args.workload, "desc": w["desc"], "capacity_slots": cap, "num_buckets": nb,
+            "table_bytes": nb * bs * bits // 8, "bits_per_tag": bits, "bucket_size": bs, "eviction": w["policy"],
+            "max_evictions": w["max_ev"], "block_size": args.block,
+            "insert_path": "insertManySorted" if sorted_fill else "insertMany",
+            "fill_keys": n_fill, "lookup_keys": w["n_pos"] + w["n_neg"], "delete_keys": w["n_del"],
+            "l2": "inputs larger than L2 (table and key arrays exceed 126 MB); no flush needed"
+            if cap >= (1 << 26) else "table L2-resident (small workload)",
+            "parallelism": f"{world} independent filter shard(s), one per GPU, no collective"}
 
 
 # ------------------------------------------------------------ GPU benchmark
@@ -362,8 +580,9 @@ def run_b200(args, w: dict) -> dict | None:
     cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=w["bits"], maxEvictions=w["max_ev"], blockSize=args.block,
                            bucketSize=w["bs"], evictionPolicy=cfb.EvictionPolicy[w["policy"]])
     f = cfb.CuckooFilter(cfg, w["capacity"])
-    f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
-    fill, query, dele, n_coll = make_inputs(w, dev, rank)
+    if args.workspace_gb is not None:
+        f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
+    fill, query, dele, n_coll, is_pos = make_inputs(w, dev, rank, with_mask=True)
     n_fill, n_q, n_d = fill.numel(), query.numel(), dele.numel()
     q_out = torch.empty(n_q, dtype=torch.bool, device=dev)
     torch.cuda.synchronize()
@@ -498,6 +717,11 @@ def run_b200(args, w: dict) -> dict | None:
             "traffic_source": traffic.get("source") if traffic else None,
             "dram_achieved": ops[dom].get("dram_gbs"), "dram_frac": ops[dom].get("dram_frac")}
 
+    # ------------------------------------- per-key parity of the timed configuration
+    if not args.no_verify:
+        acct["parity"] = verify_parity(f, w, fill, query, is_pos, dele, sorted_fill, stream)
+    del is_pos
+
     # ------------------------------------------------ end to end (host buffers)
     e2e = None
     if not args.no_e2e:
@@ -566,7 +790,11 @@ def run_b200(args, w: dict) -> dict | None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(args.cpu_scale, host_threads())
+        tab = CpuFullTable(w, fill.cpu().numpy().view(np.uint64), query.cpu().numpy().view(np.uint64),
+                           dele.cpu().numpy().view(np.uint64), host_threads())
+        tab.fill()
+        cpu = cpu_baseline_entry(tab, [tab.step(0)])
+        del tab
 
     st = f.stats()
     result = None
@@ -577,19 +805,13 @@ def run_b200(args, w: dict) -> dict | None:
             "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic: splitmix64 uint64 keys (seeded), positives sampled without replacement, "
                     "negatives disjoint by construction",
-            "config": {"workload": args.workload, "desc": w["desc"], "capacity_slots": w["capacity"],
-                       "num_buckets": f.getNumBuckets(), "table_bytes": f.sizeInBytes(),
-                       "bits_per_tag": w["bits"], "bucket_size": w["bs"], "eviction": w["policy"],
-                       "max_evictions": w["max_ev"], "block_size": args.block,
-                       "insert_path": "insertManySorted" if sorted_fill else "insertMany",
-                       "workspace_limit_gb": args.workspace_gb,
-                       "fill_keys": n_fill, "lookup_keys": n_q, "delete_keys": n_d,
-                       "negatives_replaced": n_coll,
-                       "l2": "inputs larger than L2 (table and key arrays exceed 126 MB); no flush needed"
-                       if w["capacity"] >= (1 << 26) else "table L2-resident (small workload)",
-                       "parallelism": f"{world} independent filter shard(s), one per GPU, no collective"},
+            "config": workload_config(args, w, world),
+            "library": {"workspace_limit": "library default (automatic)" if args.workspace_gb is None
+                        else f"{args.workspace_gb} GiB (CF_OPT_WORKSPACE_LIMIT)",
+                        "workspace_bytes": f.getOption(cfb.OPT_WORKSPACE_BYTES), "options": "library defaults"
+                        if args.workspace_gb is None else "CF_OPT_WORKSPACE_LIMIT set"},
             "ops": ops,
-            "accounting": {**acct, "load_factor": acct["inserted"] / f.capacity()},
+            "accounting": {**acct, "load_factor": acct["inserted"] / f.capacity(), "negatives_replaced": n_coll},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -604,6 +826,106 @@ def run_b200(args, w: dict) -> dict | None:
 
         dist.destroy_process_group()
     return result
+
+
+def verify_parity(f, w: dict, fill, query, is_pos, dele, sorted_fill: bool, stream, chunk: int = 1 << 28) -> dict:
+    """Per-key parity of the timed configuration on the full workload (untimed).
+
+    The fill is the timed steps' own (library defaults: for a large batch the
+    capped three-round segment-staged insert).  Then:
+      * counters against the image: occupied == countOccupiedSlots == stored
+        keys, lost == 0;
+      * zero false negatives over every stored fill key;
+      * the table's (bucket pair, tag) multiset equals the one the stored keys
+        must leave (digests from the torch restatement of the reference's
+        hashing, independent of the kernels);
+      * the lookup batch: every positive hits; the false positives on the
+        disjoint negatives lie within 3 sigma of the expected count (per
+        negative 1 - (1 - q)^(2 * bucketSize * load), q = sum over tags of
+        P(tag)^2 = (2^f + 2) / 2^(2f) since a zero fingerprint becomes 1);
+      * deleteMany: every deleted key reports removed, occupancy drops by
+        exactly that many, and the multiset loses exactly the deleted keys'
+        entries.
+    The reference prints 2 * bucketSize * load / 2^f as its false-positive
+    estimate (src/main.cu:458-459); it is reported beside the bound."""
+    import torch
+
+    bits, bs = w["bits"], w["bs"]
+    nb = f.getNumBuckets()
+    n_fill, n_d = fill.numel(), dele.numel()
+    dev = fill.device
+    f.clear(stream)
+    f.resetEvictionCount()
+    if sorted_fill:
+        f.insertManySorted(fill, stream=stream)
+    else:
+        f.insertMany(fill, stream=stream)
+    st = f.stats()
+    stored_mask = None
+    if st["failed"]:
+        # which keys failed: the same fill again, reporting per-key results
+        f.clear(stream)
+        f.resetEvictionCount()
+        stored_mask = torch.empty(n_fill, dtype=torch.bool, device=dev)
+        if sorted_fill:
+            f.insertManySorted(fill, stream=stream, d_output=stored_mask)
+        else:
+            f.insertMany(fill, stream=stream, d_output=stored_mask)
+        st = f.stats()
+    n_stored = n_fill - st["failed"]
+    occ, cnt = f.occupiedSlots(), f.countOccupiedSlots()
+    hit = torch.empty(min(n_fill, chunk), dtype=torch.bool, device=dev)
+    false_neg = 0
+    for a in range(0, n_fill, chunk):
+        m = min(chunk, n_fill - a)
+        f.containsManyAsync(fill[a:a + m], hit[:m], stream=stream)
+        h = hit[:m] if stored_mask is None else hit[:m] | ~stored_mask[a:a + m]
+        false_neg += int((~h).sum().item())
+    img = f.table_image()
+    dig_table = table_digest(img, bits, bs, nb)
+    del img
+    dig_keys = key_digest(fill, bits, nb, valid=stored_mask)
+    q_out = torch.empty(query.numel(), dtype=torch.bool, device=dev)
+    f.containsMany(query, q_out, stream=stream)
+    pos_missed = int((is_pos & ~q_out).sum().item())
+    n_neg = int((~is_pos).sum().item())
+    fp_hits = int((~is_pos & q_out).sum().item())
+    load = occ / f.capacity()
+    q = ((1 << bits) + 2) / float(1 << (2 * bits))
+    p_fp = 1.0 - (1.0 - q) ** (2 * bs * load)
+    expected = n_neg * p_fp
+    sigma = math.sqrt(n_neg * p_fp * (1.0 - p_fp))
+    d_out = torch.empty(n_d, dtype=torch.bool, device=dev)
+    occ_after = f.deleteMany(dele, d_out, stream=stream)
+    removed_reported = int(d_out.sum().item())
+    st_after = f.stats()
+    cnt_after = f.countOccupiedSlots()
+    multiset_after = None
+    if stored_mask is None:  # every deleted key was stored: its entry must be the one removed
+        img = f.table_image()
+        multiset_after = table_digest(img, bits, bs, nb) == digest_sub(dig_keys, key_digest(dele, bits, nb))
+        del img
+    res = {
+        "fill": "the timed steps' fill (library defaults)",
+        "stored": n_stored, "failed": st["failed"], "occupied": occ, "count_occupied_slots": cnt,
+        "lost": st["lost"], "duplicates": st["duplicates"], "counters_match_image": occ == cnt == n_stored,
+        "false_negatives_all_fill_keys": false_neg,
+        "multiset_conserved": dig_table == dig_keys, "entries_in_table": dig_table[0],
+        "lookup_positives_missed": pos_missed, "lookup_negatives": n_neg, "false_positives": fp_hits,
+        "fpr": fp_hits / max(1, n_neg), "fp_expected": expected, "fp_sigma": sigma,
+        "fp_within_3sigma": abs(fp_hits - expected) <= 3 * sigma,
+        "fpr_reference_estimate": 2 * bs * load / float(1 << bits),
+        "deleted_reported": removed_reported, "delete_keys": n_d, "removed_counter": st_after["removed"],
+        "occupied_after_delete": occ_after, "count_after_delete": cnt_after,
+        "delete_counts_match": removed_reported == n_d == st_after["removed"]
+        and occ_after == cnt_after == occ - n_d,
+        "multiset_after_delete": multiset_after,
+    }
+    res["all_passed"] = bool(
+        res["counters_match_image"] and st["lost"] == 0 and false_neg == 0 and res["multiset_conserved"]
+        and pos_missed == 0 and res["fp_within_3sigma"] and res["delete_counts_match"]
+        and multiset_after is not False)
+    return res
 
 
 def load_traffic(op: str, w: dict, path: str) -> dict | None:
@@ -976,7 +1298,8 @@ def run_grid(args) -> dict:
             cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=bits, bucketSize=bs, maxEvictions=500,
                                    evictionPolicy=cfb.EvictionPolicy[pol])
             f = cfb.CuckooFilter(cfg, base["capacity"])
-            f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
+            if args.workspace_gb is not None:
+                f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
             for path in ("insertMany", "insertManySorted"):
                 res = {}
                 for k in range(2):  # the first pass warms the workspace and the caches
@@ -1069,7 +1392,8 @@ def run_policies(args) -> dict:
         cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16, bucketSize=16, maxEvictions=500,
                                evictionPolicy=cfb.EvictionPolicy.DFS, AltBucketPolicy=name)
         f = cfb.CuckooFilter(cfg, base["capacity"])
-        f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
+        if args.workspace_gb is not None:
+            f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
         for path in ("insertMany", "insertManySorted"):
             res = {}
             for _ in range(2):  # the first pass warms the workspace and the caches
@@ -1212,28 +1536,43 @@ def run_sharded(args) -> dict | None:
 
 
 def run_reference(args, w: dict) -> dict | None:
+    """The reference arm: the reference's algorithm on the host cores (the
+    oracle's port; the reference's own CPU cuckoo library is not vendored) on
+    the workload's full-size table, all host threads and one thread; beside it,
+    where they were built from the reference's sources, the reference's own
+    CUDA kernels on the full workload on this GPU."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    threads = host_threads()
-    steps = []
-    for _ in range(args.warmup):
-        cpu_sample(args.ref_scale, threads)
-    for _ in range(args.steps):
-        steps.append(cpu_sample(args.ref_scale, threads))
-    value = statistics.mean(s["value"] for s in steps)
-    sample = steps[0]
+    import torch
+
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    fill, query, dele, _ = make_inputs(w, dev)
+    h = [t.cpu().numpy().view(np.uint64) for t in (fill, query, dele)]
+    del fill, query, dele
+    if dev.type == "cuda":
+        torch.cuda.empty_cache()
+    tab = CpuFullTable(w, h[0], h[1], h[2], host_threads())
+    tab.fill()
+    for k in range(args.warmup):
+        tab.step(k)
+    per_step = [tab.step(args.warmup + k) for k in range(args.steps)]
+    cpu = cpu_baseline_entry(tab, per_step)
+    del tab, h
+    value = cpu["value"]
+    th = cpu["threads"][str(cpu["cores"])]
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gkeys/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(s["seconds"] for s in steps) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": th["seconds_per_step"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-        "data": "synthetic: splitmix64 uint64 keys", "config": {"workload": args.workload, "desc": w["desc"]},
-        "cpu_baseline": {"value": value, "unit": "Gkeys/s", "cores": threads, "kind": "port",
-                         "sample": sample["sample"] + " (the reference's CPU cuckoo library is not vendored; "
-                                                      "this is the reference's GPU algorithm ported to host threads)"},
+        "data": "synthetic: splitmix64 uint64 keys (seeded), positives sampled without replacement, "
+                "negatives disjoint by construction",
+        "config": workload_config(args, w, 1),
+        "cpu_baseline": {**cpu, "sample": cpu["sample"] + " (the reference's CPU cuckoo library, "
+                                                          "efficient/cuckoofilter, is not vendored; this is the "
+                                                          "reference's GPU algorithm ported to host threads)"},
         "e2e": {"value": value, "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "ops": {k: statistics.mean(s[k] for s in steps) for k in ("insert_gkeys_s", "contains_gkeys_s",
-                                                                  "delete_gkeys_s")},
+        "ops": {k: th[k] for k in ("insert_gkeys_s", "contains_gkeys_s", "delete_gkeys_s")},
     }
     if not args.no_ref_gpu:
         out["reference_gpu"] = run_reference_gpu(args, w)
@@ -1257,16 +1596,17 @@ def run_reference_gpu(args, w: dict) -> dict:
     except (KeyError, RuntimeError) as e:
         return {"unavailable": f"configuration not instantiated: {e}"}
     dev = torch.device("cuda", 0)
-    fill, query, dele, _ = make_inputs(w, dev)
+    fill, query, dele, _, is_pos = make_inputs(w, dev, with_mask=True)
     out = torch.empty(query.numel(), dtype=torch.uint8, device=dev)
     res = {"ins": [], "con": [], "del": []}
+    occ_fill = 0
     stream = torch.cuda.current_stream()
     for k in range(args.warmup + args.steps):
         ref.clear()
         e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         e[0].record(stream)
-        ref.insert(fill.data_ptr(), fill.numel(), stream.cuda_stream or None,
-                   args.insert == "sorted" or (args.insert == "auto" and fill.numel() >= (1 << 29)))
+        occ_fill = ref.insert(fill.data_ptr(), fill.numel(), stream.cuda_stream or None,
+                              args.insert == "sorted" or (args.insert == "auto" and fill.numel() >= (1 << 29)))
         e[1].record(stream)
         ref.contains(query.data_ptr(), query.numel(), out.data_ptr(), stream.cuda_stream or None)
         e[2].record(stream)
@@ -1279,13 +1619,18 @@ def run_reference_gpu(args, w: dict) -> dict:
             res["del"].append(e[2].elapsed_time(e[3]))
     occ = ref.occupied()
     ref.close()
+    hits = out.to(torch.bool)
+    n_neg = int((~is_pos).sum().item())
+    fp = int((hits & ~is_pos).sum().item())
+    same_keys = {"failed_inserts": fill.numel() - int(occ_fill), "lookup_positives_missed":
+                 int((~hits & is_pos).sum().item()), "false_positives": fp, "fpr": fp / max(1, n_neg)}
     t = {k: statistics.mean(v) for k, v in res.items()}
     n_total = fill.numel() + query.numel() + dele.numel()
     return {"value": n_total / (sum(t.values()) / 1e3) / 1e9, "unit": "Gkeys/s",
             "insert_gkeys_s": fill.numel() / t["ins"] * 1e3 / 1e9,
             "contains_gkeys_s": query.numel() / t["con"] * 1e3 / 1e9,
             "delete_gkeys_s": dele.numel() / t["del"] * 1e3 / 1e9,
-            "ms": t, "occupied_after": occ,
+            "ms": t, "occupied_after": occ, "same_keys": same_keys,
             "build": "reference include/CuckooFilter.cuh compiled with -gencode arch=compute_100a,code=sm_100a "
                      "(256-bit load path live), filter object in managed memory"}
 
@@ -1301,16 +1646,17 @@ def main() -> None:
     ap.add_argument("--insert", choices=("auto", "plain", "sorted"), default="auto",
                     help="fill with insertMany (plain), insertManySorted (sorted), or as the reference's benchmark "
                          "does (auto: sorted from 2^29 keys)")
-    ap.add_argument("--workspace-gb", type=float, default=40.0,
-                    help="workspace limit of the segment-staged path (CF_OPT_WORKSPACE_LIMIT)")
+    ap.add_argument("--workspace-gb", type=float, default=None,
+                    help="workspace limit of the segment-staged path (CF_OPT_WORKSPACE_LIMIT); default: the "
+                         "library's own (automatic) limit")
+    ap.add_argument("--no-verify", action="store_true",
+                    help="skip the untimed per-key parity check of the timed configuration")
     ap.add_argument("--no-plain", action="store_true", help="skip the separate plain insertMany timing")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-chunks", type=int, default=4, help="fill chunks of the end-to-end leg (copy/compute overlap)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--cpu-scale", type=int, default=27, help="log2 slots of the CPU-baseline sample")
-    ap.add_argument("--ref-scale", type=int, default=25, help="log2 slots of each reference-arm CPU step")
     ap.add_argument("--kmer-bases-log2", type=int, default=28)
     ap.add_argument("--kmer-file", default=None,
                     help="--form kmer: insert the k-mers of this file (u64 count + u64 2-bit k-mers, the "

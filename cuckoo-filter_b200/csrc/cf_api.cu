@@ -12,7 +12,6 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 #include "../../include/cuckoo_b200.h"
@@ -39,7 +38,7 @@ struct cf_filter {
     SegGeom geom;
     void* ws;               // workspace (grown on demand, freed with the filter)
     uint64_t ws_bytes;
-    uint64_t ws_limit;      // CF_OPT_WORKSPACE_LIMIT
+    uint64_t ws_limit;      // CF_OPT_WORKSPACE_LIMIT (0 = automatic)
     uint64_t seg_min_keys;  // CF_OPT_SEGMENTED_MIN_KEYS (0 = automatic)
     uint64_t round2_min;    // CF_OPT_ROUND2_SEGMENTED_MIN_KEYS (0 = automatic)
     uint32_t round1_cap;    // CF_OPT_ROUND1_CAP (0 = automatic)
@@ -237,6 +236,25 @@ uint64_t ws_need(const cf_filter* f, uint64_t cap, int grid, bool payload) {
     return al(cap * 8) * 2 + per_key + al(hist) + al(start) + al(64);
 }
 
+// Automatic workspace limit (CF_OPT_WORKSPACE_LIMIT = 0, the default): the
+// device memory free now plus the workspace already held (it is freed before a
+// larger one is allocated), less a reserve of 1/16 of the device (at least
+// 1 GiB) left to the caller.  The reference allocates what each sorted insert
+// needs (CuckooFilter.cuh:475-508); this keeps the whole batch in one chunk
+// whenever that fits, and keeps the workspace for the next call.
+constexpr uint64_t kMinAutoWorkspace = 256ull << 20;
+
+uint64_t auto_workspace_limit(const cf_filter* f) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 4ull << 30;
+    }
+    const uint64_t reserve = std::max<uint64_t>(1ull << 30, total_b / 16);
+    const uint64_t avail = f->ws_bytes + free_b;
+    return avail > reserve + kMinAutoWorkspace ? avail - reserve : kMinAutoWorkspace;
+}
+
 int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     // radix passes: one wave of each payload mode's scatter kernel, fixed per-CTA chunks
     int rs_grid[3];
@@ -247,24 +265,41 @@ int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     const int grid = std::max(std::max(rs_grid[0], std::max(rs_grid[1], rs_grid[2])) * kRsHistSub,
                               (rg_grid * static_cast<int>(kRgMaxRegions) + kRadix - 1) / kRadix);
     const uint64_t fixed = ws_need(f, 0, grid, payload) + 4096;
-    uint64_t cap = n;
-    if (f->ws_limit > fixed) {
-        const uint64_t fit = (f->ws_limit - fixed) / (payload ? 25 : 16);
-        if (cap > fit) cap = fit;
-    } else {
-        cap = 0;
-    }
     const uint64_t kMaxChunk = 1ull << 31;  // 32-bit positions and payloads
-    if (cap > kMaxChunk) cap = kMaxChunk;
-    if (cap < n) cap = cap / 32 * 32;
-    if (cap < 1024 && n > cap) cap = 1024;
-    const uint64_t need = ws_need(f, cap, grid, payload);
-    if (f->ws_bytes < need) {
+    uint64_t limit = f->ws_limit;
+    if (limit == 0) {  // automatic: the whole batch when device memory allows
+        const uint64_t whole = ws_need(f, std::min(n, kMaxChunk), grid, payload);
+        limit = whole <= f->ws_bytes ? f->ws_bytes : auto_workspace_limit(f);
+    }
+    uint64_t cap = 0, need = 0;
+    for (;;) {
+        cap = n;
+        if (limit > fixed) {
+            const uint64_t fit = (limit - fixed) / (payload ? 25 : 16);
+            if (cap > fit) cap = fit;
+        } else {
+            cap = 0;
+        }
+        if (cap > kMaxChunk) cap = kMaxChunk;
+        if (cap < n) cap = cap / 32 * 32;
+        if (cap < 1024 && n > cap) cap = 1024;
+        need = ws_need(f, cap, grid, payload);
+        if (f->ws_bytes >= need) break;
         if (f->ws) cudaFree(f->ws);
         f->ws = nullptr;
         f->ws_bytes = 0;
-        CF_CUDA(cudaMalloc(&f->ws, need), "workspace allocation");
-        f->ws_bytes = need;
+        const cudaError_t e = cudaMalloc(&f->ws, need);
+        if (e == cudaSuccess) {
+            f->ws_bytes = need;
+            break;
+        }
+        // automatic limit: another allocation may have taken the memory since
+        // it was measured; retry with half the chunk
+        if (e != cudaErrorMemoryAllocation || f->ws_limit != 0 || need <= kMinAutoWorkspace)
+            return cuda_fail(e, "workspace allocation");
+        cudaGetLastError();
+        f->ws = nullptr;
+        limit = std::max(kMinAutoWorkspace, need / 2);
     }
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     uint8_t* p = static_cast<uint8_t*>(f->ws);
@@ -500,7 +535,7 @@ int cf_create(const cf_config* cfg, uint64_t capacity, cf_filter** out) {
     f->max_grid_aux = sms * 8;
     f->sms = sms;
     init_geometry(f);
-    f->ws_limit = 4ull << 30;
+    f->ws_limit = 0;  // automatic
     if (e == cudaSuccess) e = cudaHostAlloc(&f->h_cnt, 4 * sizeof(unsigned long long), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMalloc(&f->d_table, f->table_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&f->d_ctr, CTR_COUNT * sizeof(unsigned long long));
@@ -875,13 +910,14 @@ int cf_probe_count(cf_filter* f, const void* d_keys, uint64_t n, uint64_t* prima
 //
 // cf_insert_sorted grows a cudaMalloc'd workspace on demand and may free and
 // re-allocate it.  Some callers cannot allow that: a cudaMalloc or cudaFree
-// can synchronize the whole device (stalling other streams of a serving
-// process), allocation is not permitted while a stream is being captured, and
-// some hosts hand the library a device whose memory is already fully reserved
-// by another allocator.  For them the segment-staged insert runs here on a
-// fixed scratch area that is part of the library's own device image: a
-// file-scope __device__ array, present on every GPU on which this library's
-// code is loaded, until the process exits.  Nothing is allocated per call.
+// can synchronize the whole device (stalling the other streams of a serving
+// process), and some hosts hand the library a device whose memory is already
+// fully reserved by another allocator.  For them the segment-staged insert
+// runs here on a fixed scratch area that is part of the library's own device
+// image: a file-scope __device__ array, present on every GPU on which this
+// library's code is loaded, until the process exits.  Nothing is allocated per
+// call.  Like cf_insert_sorted, the call synchronizes its stream before it
+// returns (it reads the per-round key counts back to the host).
 
 namespace {
 
@@ -901,25 +937,18 @@ constexpr uint64_t kNaStart = na_al((kNoAllocMaxSegments + 1) * 4);
 constexpr uint64_t kNaCnt = 256;
 constexpr uint64_t kNoAllocScratchBytes = 2 * kNaEnt + 2 * kNaPay + kNaBitmap + kNaHist + kNaStart + kNaCnt;
 
-// The scratch.  In host code this name is only a handle: its device address
-// comes from cudaGetSymbolAddress, once per device (noalloc_scratch).
+// The scratch.  In host code this name is only a handle: the device address
+// comes from cudaGetSymbolAddress (noalloc_scratch).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the scratch on the current device (looked up on the
-// first call per device).
-int noalloc_scratch(int device, void** out) {
-    if (device < 0 || device >= kMaxDevices) return fail(CF_ERR_UNSUPPORTED, "device ordinal %d out of range", device);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "scratch address lookup");
-        g_noalloc_ptr[device] = p;
-    }
-    *out = g_noalloc_ptr[device];
+// Device address of the scratch on the current device.  Looked up on every
+// call (the lookup allocates nothing), so an address never outlives the
+// context it came from, e.g. across a cudaDeviceReset.
+int noalloc_scratch(void** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "scratch address lookup");
+    *out = p;
     return CF_OK;
 }
 
@@ -942,7 +971,7 @@ int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8
                     static_cast<unsigned long long>(f->geom.nseg), static_cast<unsigned long long>(kNoAllocMaxSegments));
     DeviceGuard g(f->device);
     void* base = nullptr;
-    if (int s = noalloc_scratch(f->device, &base)) return s;
+    if (int s = noalloc_scratch(&base)) return s;
     SegWork w{};
     CF_CUDA(rs_scatter_grid<0>(f->sms, &w.rs_grid[0]), "radix launch setup");
     CF_CUDA(rs_scatter_grid<1>(f->sms, &w.rs_grid[1]), "radix launch setup");

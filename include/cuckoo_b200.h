@@ -188,8 +188,14 @@ int cf_load_table(cf_filter* f, const void* src, uint64_t bytes, void* stream);
 
 /* Tunables of a filter (cf_set_option / cf_get_option). */
 typedef enum cf_option {
-    /* Upper bound on the device workspace of the segment-staged path, in bytes
-     * (default 4 GiB).  Larger batches are processed in chunks that fit. */
+    /* Upper bound on the device workspace of the staged paths, in bytes.
+     * 0 (default) = automatic: a batch gets a workspace for all of it (16
+     * bytes per key, 25 with per-key results, up to 2^31 keys per chunk) when
+     * the device's free memory, less a reserve of 1/16 of the device, allows,
+     * else the largest chunk that fits.  The reference allocates the sorted
+     * insert's buffers inside every call (CuckooFilter.cuh:475-508); here the
+     * workspace is kept for later calls and freed with the filter.  Larger
+     * batches than the limit are processed in chunks that fit. */
     CF_OPT_WORKSPACE_LIMIT = 1,
     /* Batch size from which insertMany, containsMany and deleteMany stream
      * table segments through shared memory instead of probing at random
@@ -286,22 +292,23 @@ int cf_alt_buckets(const cf_config* cfg, uint64_t num_buckets, const uint64_t* b
  *
  * cf_insert_sorted grows a workspace with cudaMalloc and may free it again.
  * A process that serves many streams cannot let a call do that (cudaMalloc
- * and cudaFree can synchronize the whole device), a stream being captured into
- * a CUDA graph may not allocate, and a host whose device memory is reserved by
- * another allocator has none to give.  This entry point runs the same
- * segment-staged insert on a fixed scratch area built into the library
- * (cf_noalloc_scratch_bytes(), about 27 MiB), which every GPU that loads the
- * library's device code holds until the process exits.  It calls no
- * cudaMalloc, cudaFree or allocating routine.
+ * and cudaFree can synchronize the whole device and stall every other
+ * stream), and a host whose device memory is reserved by another allocator
+ * has none to give.  This entry point runs the same segment-staged insert on
+ * a fixed scratch area built into the library (cf_noalloc_scratch_bytes(),
+ * about 27 MiB), which every GPU that loads the library's device code holds
+ * until the process exits.  It calls no cudaMalloc, cudaFree or allocating
+ * routine; each call looks up the scratch's device address on the filter's
+ * device with cudaGetSymbolAddress, which allocates nothing.
  *
  * Limits: at most CF_NOALLOC_MAX_KEYS keys per call (larger n returns
  * CF_ERR_INVALID; split the batch), tables of at most 2^18 segments of 64 KiB
- * (16 GiB; else CF_ERR_UNSUPPORTED).  The first call on a device looks up the
- * scratch address there; make that first call before any stream capture.
- * All calls share the one scratch area: calls that overlap on the GPU (other
- * streams, other threads, other filters) race and must be serialized by the
- * caller.  Contract otherwise as cf_insert_sorted (synchronous; d_out and
- * occupied_out optional).
+ * (16 GiB; else CF_ERR_UNSUPPORTED).  All calls share the one scratch area
+ * and each call leaves its contents behind (every call rewrites what it
+ * reads before reading it): calls that overlap on the GPU (other streams,
+ * other threads, other filters) race and must be serialized by the caller.
+ * Contract otherwise as cf_insert_sorted: d_out and occupied_out optional,
+ * and the call synchronizes `stream` before it returns.
  */
 #define CF_NOALLOC_MAX_KEYS (1u << 20)
 int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream,

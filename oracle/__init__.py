@@ -12,7 +12,7 @@ Three native pieces are wrapped here:
   used as the CPU baseline.
 * ``_ref/libref_host.so`` -- the reference's own ``XorAltBucketPolicy`` and
   ``xxhash64`` compiled from its headers (pins the restatement's hashing).
-* ``_ref/libref_gpu.so`` -- the reference's own CUDA kernels (GPU box only).
+* ``_ref/libref_gpu.so`` -- the reference's own CUDA kernels (run only where a GPU is present).
 """
 from __future__ import annotations
 

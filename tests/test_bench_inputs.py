@@ -1,4 +1,4 @@
-"""Host logic of bench.py: key generators and disjointness (CPU only)."""
+"""Host logic of bench.py: key generators, disjointness and the parity check's hashing and digests (CPU only)."""
 from __future__ import annotations
 
 import numpy as np
@@ -102,3 +102,69 @@ def test_markov_dna_and_mutation_cpu():
     m = bench.mutate(dna, 0.01, seed=2)
     diff = (m != dna).float().mean().item()
     assert 0.0 < diff < 0.03
+
+
+# ------------------------------------- the parity check's hashing and digests
+
+
+def test_parity_hashing_matches_reference_golden(golden):
+    """bench.py's torch restatement of xxHash64 and XorAltBucketPolicy against the
+    vectors generated from the reference's own hashutil.cuh / bucket_policies.cuh."""
+    for i in range(10):
+        kb, bits, _bs, _cap, nb = (int(x) for x in golden[f"c{i}_meta"])
+        keys = golden[f"c{i}_keys"]
+        kt = torch.from_numpy(keys.view(np.int64) if keys.dtype == np.uint64 else keys.astype(np.int64))
+        h = bench.xxh64_torch(kt, kb).numpy().view(np.uint64)
+        assert np.array_equal(h, golden[f"c{i}_hash"]), i
+        i1, i2, fp = bench.candidates_torch(kt, kb, bits, nb, bench.tag_hash_table(bits, "cpu") if bits <= 16 else None)
+        assert np.array_equal(i1.numpy().view(np.uint64), golden[f"c{i}_i1"]), i
+        assert np.array_equal(i2.numpy().view(np.uint64), golden[f"c{i}_i2"]), i
+        assert np.array_equal(fp.numpy().astype(np.uint32), golden[f"c{i}_fp"]), i
+    for b in (8, 16, 32):
+        t = torch.from_numpy(golden[f"tag{b}"].astype(np.int64))
+        assert np.array_equal(bench.xxh64_torch(t, b // 8).numpy().view(np.uint64), golden[f"taghash{b}"]), b
+
+
+def _oracle_filled(orc, bits, seed=5):
+    o = orc.OracleFilter(key_bytes=8, bits=bits, bucket_size=16, policy=orc.POLICY_BFS, capacity=1 << 16)
+    keys = orc.splitmix64(seed, int(0.95 * (1 << 16)))
+    _, ok = o.insert(keys, out=True)
+    return o, keys, ok.astype(bool)
+
+
+def test_digests_agree_on_an_oracle_table(orc):
+    for bits in (8, 16):
+        o, keys, ok = _oracle_filled(orc, bits)
+        kt = torch.from_numpy(keys.view(np.int64))
+        stored = bench.key_digest(kt, bits, o.nb, valid=torch.from_numpy(ok), chunk=1 << 12)
+        table = bench.table_digest(torch.from_numpy(o.table), bits, 16, o.nb, chunk_slots=1 << 12)
+        assert stored == table and stored[0] == o.occupied() == int(ok.sum()), bits
+        # deleting a subset removes exactly its entries from the multiset
+        gone = keys[ok][:5000]
+        n, _ = o.delete(gone)
+        assert n == 5000
+        after = bench.table_digest(torch.from_numpy(o.table), bits, 16, o.nb)
+        assert after == bench.digest_sub(stored, bench.key_digest(torch.from_numpy(gone.view(np.int64)), bits, o.nb))
+
+
+def test_digest_catches_a_planted_mistake_in_the_oracle_table(orc):
+    o, keys, ok = _oracle_filled(orc, 16)
+    want = bench.key_digest(torch.from_numpy(keys.view(np.int64)), 16, o.nb, valid=torch.from_numpy(ok))
+    slots = o.slots()
+    b, s = np.argwhere(slots != 0)[123]
+    # a tag moved to a bucket that is neither of its key's candidates
+    moved = o.table.copy()
+    mv = moved.view(np.uint16).reshape(o.nb, 16)
+    free = np.argwhere(mv[(b + 1) % o.nb] == 0)
+    if len(free):
+        mv[(b + 1) % o.nb, free[0][0]] = mv[b, s]
+        mv[b, s] = 0
+        assert bench.table_digest(torch.from_numpy(moved), 16, 16, o.nb) != want
+    # a tag changed in place
+    changed = o.table.copy()
+    changed.view(np.uint16).reshape(o.nb, 16)[b, s] ^= 1
+    assert bench.table_digest(torch.from_numpy(changed), 16, 16, o.nb) != want
+    # a tag dropped
+    dropped = o.table.copy()
+    dropped.view(np.uint16).reshape(o.nb, 16)[b, s] = 0
+    assert bench.table_digest(torch.from_numpy(dropped), 16, 16, o.nb) != want

@@ -1,7 +1,7 @@
 """The N>1 path of bench.py on CPU: two gloo ranks, each an independent filter
 shard with its own key streams, aggregated as the whole job (keys of all
 ranks over the slowest rank's time).  No GPU and no NCCL: the reductions run
-over gloo exactly as they run over NCCL on the GPU box."""
+over gloo exactly as they run over NCCL on GPUs."""
 from __future__ import annotations
 
 import os

@@ -1,0 +1,145 @@
+"""Insert failures and false positives against the reference's own kernels.
+
+The reference's CUDA kernels (built from its sources for sm_100a into
+oracle/_ref/libref_gpu.so) and this library take the same keys, and the
+figures that concurrency makes random are compared as binomial counts: the
+insert-failure count and the false-positive count on disjoint negative keys
+must agree within 3 sigma of their difference.  The flow is the reference's
+own example (src/main.cu:85-175): insert, query the keys and as many
+negatives, delete the first half, query again.
+
+Where the two insert paths are different algorithms (this library's
+segment-staged insert fills in capped rounds before it evicts), the failure
+count is held one-sided: no more failures than the reference plus 3 sigma.
+
+Under overload, eviction walks that run concurrently can cross.  The
+reference then drops the tag in hand at every failed walk (CuckooFilter.cuh:
+953), so each of its failures leaves one key absent; this library undoes a
+failed walk and counts the rare tag it cannot put back as `lost`.  The keys
+absent after the fill (failed + lost here, failed there) are what is compared.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+from test_gpu_parity import STAGING, dev, host_u8  # noqa: E402
+
+
+def _sigma_diff(a: int, b: int, n: int) -> float:
+    """Standard deviation of the difference of two independent binomial counts
+    over n trials with the pooled rate (a + b) / 2n."""
+    p = (a + b) / (2.0 * n)
+    return math.sqrt(2.0 * n * p * (1.0 - p))
+
+
+def _run_ours(cfb, cfg, capacity, keys, neg, path, staging):
+    f = cfb.CuckooFilter(cfg, capacity)
+    try:
+        f.setOption(cfb.OPT_STAGING, STAGING[staging])
+        d = dev(keys)
+        ok_t = torch.empty(len(keys), dtype=torch.bool, device="cuda")
+        (f.insertManySorted if path == "sorted" else f.insertMany)(d, d_output=ok_t)
+        ok = host_u8(ok_t).astype(bool)
+        st = f.stats()
+        assert st["failed"] == len(keys) - ok.sum()
+        assert f.occupiedSlots() == f.countOccupiedSlots() == len(keys) - st["failed"] - st["lost"]
+        fp1 = int(host_u8(f.containsMany(dev(neg))).sum())
+        stored = keys[ok]
+        half = stored[: len(stored) // 2]
+        out = torch.empty(len(half), dtype=torch.bool, device="cuda")
+        f.deleteMany(dev(half), out)
+        removed = int(host_u8(out).sum())
+        fn_rest = int((~host_u8(f.containsMany(dev(stored[len(half):]))).astype(bool)).sum())
+        fp2 = int(host_u8(f.containsMany(dev(neg))).sum())
+        return {"failed": int(st["failed"]), "lost": int(st["lost"]), "absent": int(st["failed"] + st["lost"]),
+                "fp": fp1, "removed": removed, "half": len(half), "fn_after_delete": fn_rest,
+                "fp_after_delete": fp2}
+    finally:
+        f.close()
+
+
+def _run_ref(orc, key, capacity, keys, neg, sorted_):
+    ref = orc.RefGpuFilter(*key, capacity)
+    try:
+        d = dev(keys)
+        occ = int(ref.insert(d.data_ptr(), len(keys), None, sorted_))
+        q = dev(neg)
+        out = torch.zeros(len(neg), dtype=torch.uint8, device="cuda")
+        ref.contains(q.data_ptr(), len(neg), out.data_ptr())
+        fp1 = int(out.sum().item())
+        half = keys[: len(keys) // 2]
+        ref.delete(dev(half).data_ptr(), len(half), None)
+        out.zero_()
+        ref.contains(q.data_ptr(), len(neg), out.data_ptr())
+        return {"failed": len(keys) - occ, "absent": len(keys) - occ, "fp": fp1,
+                "fp_after_delete": int(out.sum().item())}
+    finally:
+        ref.close()
+
+
+@pytest.fixture(scope="module")
+def small_config(orc):
+    """The small configuration: 2^20 slots, 996 147 keys (splitmix64 seed 1), as
+    many negatives (seed 2) with any collision with a key removed."""
+    keys = orc.splitmix64(1, 996147)
+    neg = orc.splitmix64(2, 996147)
+    return keys, neg[~np.isin(neg, keys)]
+
+
+@pytest.mark.parametrize("path,staging", [("plain", "auto"), ("plain", "random"), ("sorted", "auto")])
+def test_small_config_matches_reference_kernels_statistically(cfb, orc, small_config, path, staging):
+    if orc.ref_gpu() is None:
+        pytest.skip("oracle/_ref/libref_gpu.so not built")
+    keys, neg = small_config
+    cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16, maxEvictions=500, blockSize=256, bucketSize=16,
+                           evictionPolicy=cfb.EvictionPolicy.BFS)
+    mine = _run_ours(cfb, cfg, 1 << 20, keys, neg, path, staging)
+    ref = _run_ref(orc, (8, 16, 16, orc.POLICY_BFS, 500), 1 << 20, keys, neg, path == "sorted")
+    n, m = len(keys), len(neg)
+    msg = f"ours {mine} reference {ref}"
+    assert mine["lost"] == 0, msg
+    assert abs(mine["failed"] - ref["failed"]) <= 3 * _sigma_diff(mine["failed"], ref["failed"], n) + 3, msg
+    assert abs(mine["fp"] - ref["fp"]) <= 3 * _sigma_diff(mine["fp"], ref["fp"], m) + 3, msg
+    assert abs(mine["fp_after_delete"] - ref["fp_after_delete"]) <= \
+        3 * _sigma_diff(mine["fp_after_delete"], ref["fp_after_delete"], m) + 3, msg
+    # deleteMany removes exactly one copy per stored key and keeps the others
+    assert mine["removed"] == mine["half"] and mine["fn_after_delete"] == 0, msg
+    # the reference's printed estimate 2 * b * load / 2^f (src/main.cu:458-459), as a sanity band
+    est = 2 * 16 * 0.95 / 2 ** 16
+    assert 0.8 * est < mine["fp"] / m < 1.2 * est, msg
+
+
+@pytest.mark.parametrize("policy", ["BFS", "DFS"])
+@pytest.mark.parametrize("path,staging", [("plain", "random"), ("sorted", "auto")])
+def test_failures_under_overload_against_reference_kernels(cfb, orc, policy, path, staging):
+    """2^16 slots, maxEvictions 16, 0.995 x capacity keys: thousands of inserts
+    fail in both.  The random path is the reference's own algorithm (two-sided
+    3 sigma); the segment-staged path may only fail less."""
+    if orc.ref_gpu() is None:
+        pytest.skip("oracle/_ref/libref_gpu.so not built")
+    cap = 1 << 16
+    keys = orc.splitmix64(77, int(0.995 * cap))
+    neg = orc.splitmix64(78, 200_000)
+    neg = neg[~np.isin(neg, keys)]
+    pol = orc.POLICY_BFS if policy == "BFS" else orc.POLICY_DFS
+    cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16, maxEvictions=16, bucketSize=16,
+                           evictionPolicy=cfb.EvictionPolicy[policy])
+    mine = _run_ours(cfb, cfg, cap, keys, neg, path, staging)
+    ref = _run_ref(orc, (8, 16, 16, pol, 16), cap, keys, neg, path == "sorted")
+    n = len(keys)
+    s = 3 * _sigma_diff(mine["absent"], ref["absent"], n) + 3
+    msg = f"ours {mine} reference {ref}"
+    assert ref["absent"] > 0, msg
+    if staging == "random":
+        assert abs(mine["absent"] - ref["absent"]) <= s, msg
+    else:
+        assert mine["absent"] <= ref["absent"] + s, msg
+    # a lost tag belonged to some key reported stored: at most that many of
+    # them can fail to delete or go missing afterwards
+    assert mine["removed"] >= mine["half"] - mine["lost"] and mine["fn_after_delete"] <= mine["lost"], msg
