@@ -1409,6 +1409,168 @@ def run_policies(args) -> dict:
                                    "keys), 2^28 lookups 50% positive, 2^26 deletes"}, "rows": rows}
 
 
+def sharded_step(f, fill, query, dele, marks=None) -> tuple:
+    """One step of the plain workload through the hash-partitioned front end
+    (CuckooFilterMultiGPU): every rank inserts its own fill keys, looks up its
+    own query batch and deletes its own delete batch; keys travel to the rank
+    that owns them and results come back in the caller's order.  `marks`, if
+    given, is called between the phases (0 before the insert, 1, 2 and 3 after
+    each phase) to record timing events.  Returns (lookup results, per-key
+    delete results) aligned with `query` and `dele`."""
+    if marks:
+        marks(0)
+    f.insertMany(fill)
+    if marks:
+        marks(1)
+    q_out = f.containsMany(query)
+    if marks:
+        marks(2)
+    d_out = f.torch.empty(dele.numel(), dtype=f.torch.bool, device=q_out.device)
+    f.deleteMany(dele, d_out)
+    if marks:
+        marks(3)
+    return q_out, d_out
+
+
+def sharded_capacity(world: int, slots_per_rank: int) -> int:
+    """Total capacity of CuckooFilterMultiGPU that gives each of `world` ranks
+    a shard of `slots_per_rank` slots: the per-GPU capacity
+    SDIV(capacity, N) * 1.02 (CuckooFilterMultiGPU.cuh:337) stays within one
+    power-of-two bucket count."""
+    return int(world * (slots_per_rank - 64) / 1.02)
+
+
+def run_b200_sharded(args, w: dict) -> dict | None:
+    """The plain workload on N GPUs through the hash-partitioned front end
+    (cuckoo-filter_b200/multigpu.py; the reference's CuckooFilterMultiGPU,
+    CuckooFilterMultiGPU.cuh:168-322): each rank brings the workload's batch
+    (its own key streams, seeds offset by rank), keys are grouped on the device
+    and exchanged with NCCL all-to-all, each rank's shard of the workload's
+    capacity runs the batch operation, and lookup and delete results come back
+    in batch order.  Weak scaling: N shards of the workload's size."""
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    import cuckoo_b200.multigpu as mg
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    own_group = False
+    import torch.distributed as dist
+
+    if not dist.is_initialized():  # one rank without torchrun: a group of one
+        import datetime
+        import socket
+
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", str(port))
+        dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        own_group = True
+    world = dist.get_world_size()
+    stream = torch.cuda.current_stream()
+    cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=w["bits"], maxEvictions=w["max_ev"], blockSize=args.block,
+                           bucketSize=w["bs"], evictionPolicy=cfb.EvictionPolicy[w["policy"]])
+    f = mg.CuckooFilterMultiGPU(cfg, sharded_capacity(world, w["capacity"]), routing=args.routing,
+                                max_keys_per_call=1 << 31)
+    fill, query, dele, _, is_pos = make_inputs(w, dev, rank, with_mask=True)
+    n_fill, n_q, n_d = fill.numel(), query.numel(), dele.numel()
+    for _ in range(args.warmup):
+        f.clear()
+        sharded_step(f, fill, query, dele)
+    torch.cuda.synchronize()
+    phases = []
+    launches0 = cfb.launch_count()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            f.clear()
+            barrier(world)
+            torch.cuda.synchronize()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            q_out, d_out = sharded_step(f, fill, query, dele, marks=lambda i: ev[i].record(stream))
+            torch.cuda.synchronize()
+            phases.append([ev[i].elapsed_time(ev[i + 1]) for i in range(3)])
+    launches = cfb.launch_count() - launches0
+    # the last step's results: every positive found, every delete removed
+    pos_missed = int((is_pos & ~q_out).sum().item())
+    fp = int((~is_pos & q_out).sum().item())
+    removed = int(d_out.sum().item())
+    st = f.ops.filter.stats()
+    failed = int(_reduce(world, float(st["failed"] + st["lost"]), "sum"))
+    total_ms = max_over_ranks(world, sum(sum(p) for p in phases))
+    ph = [max_over_ranks(world, statistics.mean(p[i] for p in phases)) for i in range(3)]
+    keys_per_step = n_fill + n_q + n_d
+    all_keys = sum_over_ranks(world, keys_per_step * args.steps)
+    value = all_keys / (total_ms / 1e3) / 1e9
+    peak, peak_src = measured_peak()
+    # the rank's own shard: inserts of the keys it received, 72 B each (no primary-full credit)
+    recv = st["primary"] + st["secondary"] + st["evicted_inserts"]  # the last step's (cleared each step)
+    ins_bytes = 72 * recv
+    ok = sum_over_ranks(world, float(pos_missed == 0 and removed == n_d and failed == 0))
+    # end to end: every step copies the rank's inputs from pinned host memory
+    # into the device buffers and the lookup results back
+    e2e = None
+    if not args.no_e2e:
+        hosts = [pinned_empty(t.numel(), t.dtype) for t in (fill, query, dele)]
+        h_out = pinned_empty(n_q, torch.bool)
+        for h, t in zip(hosts, (fill, query, dele)):
+            h.copy_(t)
+        times = []
+        for k in range(max(1, min(args.steps, args.e2e_steps)) + 1):
+            f.clear()
+            barrier(world)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for h, t in zip(hosts, (fill, query, dele)):
+                t.copy_(h, non_blocking=True)
+            q_e, _ = sharded_step(f, fill, query, dele)
+            h_out.copy_(q_e)
+            torch.cuda.synchronize()
+            if k:
+                times.append(time.perf_counter() - t0)
+        t = max_over_ranks(world, statistics.mean(times))
+        del hosts, h_out
+        release_pinned()
+        e2e = {"value": all_keys / args.steps / t / 1e9, "unit": "Gkeys/s",
+               "h2d_bytes_per_step": 8 * keys_per_step * world, "d2h_bytes_per_step": n_q * world,
+               "ms_per_step": t * 1e3, "steps": len(times),
+               "path": "CuckooFilterMultiGPU insertMany / containsMany / deleteMany on every rank; inputs copied "
+                       "from pinned host memory, lookup results copied back; wall clock per step, max over ranks"}
+    result = None
+    if rank == 0:
+        result = {
+            "metric": METRIC, "value": value, "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: splitmix64 uint64 keys (seeded per rank), positives sampled without replacement, "
+                    "negatives disjoint by construction",
+            "config": {**workload_config(args, w, world),
+                       "parallelism": f"{world} hash-partitioned shards of {w['capacity']} slots "
+                                      f"(CuckooFilterMultiGPU, {args.routing} routing), keys and results "
+                                      "exchanged with NCCL all-to-all"},
+            "ops": {"insert": {"ms": ph[0], "gkeys_s": world * n_fill / ph[0] / 1e6},
+                    "contains": {"ms": ph[1], "gkeys_s": world * n_q / ph[1] / 1e6},
+                    "delete": {"ms": ph[2], "gkeys_s": world * n_d / ph[2] / 1e6}},
+            "roofline": {"bound": "hbm", "kernel": "insert phase on rank 0's shard (grouping, exchange and "
+                                                  "the shard's insertMany)",
+                         "achieved": ins_bytes / (ph[0] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": ins_bytes / (ph[0] / 1e3) / 1e9 / peak, "peak_source": peak_src,
+                         "traffic": None},
+            "accounting": {"ranks_all_checks_passed": int(ok), "positives_missed_rank0": pos_missed,
+                           "false_positives_rank0": fp, "removed_rank0": removed, "absent_inserts_all": failed},
+            "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+    del f
+    if own_group:
+        dist.destroy_process_group()
+    return result
+
+
 def run_sharded(args) -> dict | None:
     """The hash-partitioned multi-GPU form (CuckooFilterMultiGPU: one rank per
     GPU, keys grouped on the device and exchanged with NCCL all-to-all).  The
@@ -1532,6 +1694,152 @@ def run_sharded(args) -> dict | None:
     return out
 
 
+# ------------------------------------------------------- lookup-ceiling measurements
+
+
+def run_gather(args) -> dict:
+    """DRAM cost of random 32-byte bucket probes, for an ncu capture of one
+    launch: 2^24 keys each load their primary bucket once (k_probe_count,
+    through cf_probe_count) from a 1 GiB table (2^29 slots, 16-bit tags,
+    16-slot buckets: 2^25 buckets of 32 bytes).  Besides the probes the kernel
+    streams only the keys (8 bytes each)."""
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=16, bucketSize=16, evictionPolicy=cfb.EvictionPolicy.BFS)
+    f = cfb.CuckooFilter(cfg, 1 << 29)
+    n = 1 << 24
+    keys = torch.empty(n, dtype=torch.int64, device=dev)
+    splitmix64_torch(21, 0, n, keys)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        f.probe_count(keys, stream=stream)
+    ms = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f.probe_count(keys, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    out = {"form": "gather", "metric": "random 32-byte bucket probes per second (k_probe_count)", "unit": "Gprobes/s",
+           "value": n / statistics.median(ms) / 1e6, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "config": {"workload": "gather: 2^24 keys, one primary-bucket probe each, 1 GiB table (2^25 buckets "
+                                  "of 32 B)", "probes": n, "table_bytes": f.sizeInBytes()},
+           "ms_call_median": statistics.median(ms),
+           "note": "the call includes a counter allocation and read-back; per-probe DRAM bytes come from the ncu "
+                   "capture of the kernel alone"}
+    f.close()
+    return out
+
+
+def run_lookup_paths(args, w: dict) -> dict:
+    """Lookups and deletes of the workload on each execution path, on the same
+    filled table: random probes, segment-staged and region-staged
+    (CF_OPT_STAGING), CUDA events per call, with the lookup results required
+    to be identical across paths and every delete to succeed."""
+    import torch
+
+    from __graft_entry__ import package
+
+    cfb = package()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    cfg = cfb.CuckooConfig(T="uint64_t", bitsPerTag=w["bits"], maxEvictions=w["max_ev"], bucketSize=w["bs"],
+                           evictionPolicy=cfb.EvictionPolicy[w["policy"]])
+    f = cfb.CuckooFilter(cfg, w["capacity"])
+    fill, query, dele, _ = make_inputs(w, dev)
+    stream = torch.cuda.current_stream()
+    f.insertManySorted(fill, stream=stream)
+    del fill
+    torch.cuda.empty_cache()
+    q_out = torch.empty(query.numel(), dtype=torch.bool, device=dev)
+    d_out = torch.empty(dele.numel(), dtype=torch.bool, device=dev)
+    ref_out = None
+    rows = []
+    peak, _ = measured_peak()
+    for name, mode in (("random probes", cfb.STAGING_RANDOM), ("segment-staged", cfb.STAGING_SEGMENT),
+                       ("region-staged", cfb.STAGING_REGION)):
+        f.setOption(cfb.OPT_STAGING, mode)
+        con, dl = [], []
+        for k in range(args.warmup + args.steps):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            f.containsManyAsync(query, q_out, stream=stream)
+            e[1].record(stream)
+            f.deleteManyAsync(dele, d_out, stream=stream)
+            e[2].record(stream)
+            torch.cuda.synchronize()
+            removed = int(d_out.sum().item())
+            f.setOption(cfb.OPT_STAGING, cfb.STAGING_AUTO)
+            f.insertMany(dele, stream=stream)  # put the deleted keys back (untimed)
+            f.setOption(cfb.OPT_STAGING, mode)
+            if k >= args.warmup:
+                con.append(e[0].elapsed_time(e[1]))
+                dl.append(e[1].elapsed_time(e[2]))
+        if ref_out is None:
+            ref_out = q_out.clone()
+        q_primary = f.probe_count(query, stream=stream)
+        con_bytes = query.numel() * 9 + 32 * (2 * query.numel() - q_primary)
+        rows.append({"path": name, "contains_ms": statistics.median(con),
+                     "contains_gkeys_s": query.numel() / statistics.median(con) / 1e6,
+                     "contains_frac_sector_roofline": con_bytes / (statistics.median(con) / 1e3) / 1e9 / peak,
+                     "delete_ms": statistics.median(dl), "delete_gkeys_s": dele.numel() / statistics.median(dl) / 1e6,
+                     "lookups_identical_to_random": bool(torch.equal(q_out, ref_out)),
+                     "deletes_all_removed": removed == dele.numel()})
+        print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    f.close()
+    return {"form": "lookup_paths", "metric": "lookup and delete Gkeys/s per execution path", "unit": "Gkeys/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "dtype": "u64",
+            "data": "synthetic: splitmix64 keys", "config": {"workload": args.workload, "desc": w["desc"]},
+            "rows": rows}
+
+
+# ------------------------------------------------------------ forms summary
+
+
+def run_forms_summary(args) -> dict:
+    """The batched and served forms in brief, for the default bench line:
+    the batched form over 1024 uneven filters (the 4096-filter workload's
+    distributions; the full form is --form batched) against a loop of plain
+    per-filter calls, and the served form at an offered 200 Mkeys/s for
+    0.25 s of arrivals against a FIFO of plain per-request calls (the full
+    sweep is --form served)."""
+    import copy
+
+    import torch
+
+    a = copy.copy(args)
+    a.filters, a.steps, a.warmup = 1024, 3, 1
+    b = run_batched(a)
+    torch.cuda.empty_cache()
+    a = copy.copy(args)
+    a.loads, a.duration = "200", 0.25
+    sv = run_served(a)
+    torch.cuda.empty_cache()
+    ld = sv["loads"][0]
+    return {
+        "batched": {"workload": f"{b['config']['filters']} filters, capacities log-uniform 2^10..2^22 slots, 16/16; "
+                                "batches lognormal(ln 20000, 1.5); one persistent insert launch, lookups from one "
+                                "captured graph",
+                    "gkeys_s": b["value"], "insert_gkeys_s": b["set"]["insert_gkeys_s"],
+                    "lookup_gkeys_s": b["set"]["lookup_gkeys_s"], "plain_loop_gkeys_s": b["loop_baseline"]["value"],
+                    "speedup_vs_plain_loop": b["speedup_vs_loop"],
+                    "same_hits": b["set"]["hits"] == b["loop_baseline"]["hits"]},
+        "served": {"workload": "256 tenants, Poisson arrivals at 200 Mkeys/s offered for 0.25 s, 60/30/10 "
+                               "lookup/insert/delete",
+                   "p50_ms": ld["served"]["p50_ms"], "p99_ms": ld["served"]["p99_ms"],
+                   "mkeys_s": ld["served"]["throughput_mkeys_s"],
+                   "plain_fifo": {"p50_ms": ld["plain_fifo"]["p50_ms"], "p99_ms": ld["plain_fifo"]["p99_ms"],
+                                  "mkeys_s": ld["plain_fifo"]["throughput_mkeys_s"]},
+                   "results_identical": ld["results_identical"]},
+    }
+
+
 # ------------------------------------------------------------ reference arm
 
 
@@ -1649,6 +1957,8 @@ def main() -> None:
     ap.add_argument("--workspace-gb", type=float, default=None,
                     help="workspace limit of the segment-staged path (CF_OPT_WORKSPACE_LIMIT); default: the "
                          "library's own (automatic) limit")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the brief batched / served forms in the default line")
     ap.add_argument("--no-verify", action="store_true",
                     help="skip the untimed per-key parity check of the timed configuration")
     ap.add_argument("--no-plain", action="store_true", help="skip the separate plain insertMany timing")
@@ -1661,13 +1971,19 @@ def main() -> None:
     ap.add_argument("--kmer-file", default=None,
                     help="--form kmer: insert the k-mers of this file (u64 count + u64 2-bit k-mers, the "
                          "reference's k-mer benchmark format) instead of synthetic DNA")
-    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid", "policies", "sharded"),
+    ap.add_argument("--form", choices=("plain", "batched", "served", "kmer", "grid", "policies", "sharded", "gather",
+                                       "lookup_paths"),
                     default="plain",
                     help="batched: the filter-set form over 4096 uneven filters; served: the multi-tenant "
                          "continuous-batching form; sharded: the hash-partitioned multi-GPU form (each its own "
                          "JSON line)")
-    ap.add_argument("--routing", choices=("reference", "remixed"), default="reference",
-                    help="--form sharded: shard routing of CuckooFilterMultiGPU")
+    ap.add_argument("--routing", choices=("reference", "remixed"), default=None,
+                    help="shard routing of CuckooFilterMultiGPU (default: reference for --form sharded, remixed for "
+                         "the plain form on N GPUs)")
+    ap.add_argument("--multi", choices=("auto", "sharded", "independent"), default="auto",
+                    help="plain form on N GPUs: 'sharded' = one filter hash-partitioned over the GPUs "
+                         "(CuckooFilterMultiGPU, NCCL all-to-all), 'independent' = one independent filter per GPU "
+                         "with no collective; auto = sharded for N > 1, the single filter for N = 1")
     ap.add_argument("--shard-slots-log2", type=int, default=28, help="--form sharded: log2 slots per rank")
     ap.add_argument("--tenants", type=int, default=256)
     ap.add_argument("--loads", default="10,50,100,200", help="offered loads of the served form, Mkeys/s")
@@ -1690,9 +2006,24 @@ def main() -> None:
     elif args.form == "grid":
         res = run_grid(args)
     elif args.form == "sharded":
+        args.routing = args.routing or "reference"
         res = run_sharded(args)
+    elif args.form == "gather":
+        res = run_gather(args)
+    elif args.form == "lookup_paths":
+        res = run_lookup_paths(args, w)
+    elif args.impl == "reference":
+        res = run_reference(args, w)
     else:
-        res = run_reference(args, w) if args.impl == "reference" else run_b200(args, w)
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        sharded = args.multi == "sharded" or (args.multi == "auto" and world > 1)
+        if sharded:
+            args.routing = args.routing or "remixed"
+            res = run_b200_sharded(args, w)
+        else:
+            res = run_b200(args, w)
+            if res is not None and world == 1 and not args.no_forms:
+                res["forms"] = run_forms_summary(args)
     if res is not None:
         print(json.dumps(res), flush=True)
 

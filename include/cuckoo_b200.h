@@ -190,7 +190,7 @@ int cf_load_table(cf_filter* f, const void* src, uint64_t bytes, void* stream);
 typedef enum cf_option {
     /* Upper bound on the device workspace of the staged paths, in bytes.
      * 0 (default) = automatic: a batch gets a workspace for all of it (16
-     * bytes per key, 25 with per-key results, up to 2^31 keys per chunk) when
+     * bytes per key, about 24 with per-key results, up to 2^31 keys per chunk) when
      * the device's free memory, less a reserve of 1/16 of the device, allows,
      * else the largest chunk that fits.  The reference allocates the sorted
      * insert's buffers inside every call (CuckooFilter.cuh:475-508); here the
