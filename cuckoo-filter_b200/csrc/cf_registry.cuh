@@ -307,28 +307,57 @@ struct Launchers {
     // (w.cnt[3] for round 3; w.cnt[2] is the eviction list's).
     static constexpr uint32_t round1_cap() { return C::bs - C::bs * kRound1SlackSixteenths / 16; }
 
+    // Every kernel of a segment round has this signature (k_seg and k_seg_insert).
+    using SegKernel = void (*)(DevTable, const uint64_t*, const uint32_t*, const uint32_t*, uint64_t, int, int,
+                               uint64_t*, uint32_t*, unsigned long long*, uint32_t*, int, uint32_t, int);
+
+    // The k_seg_insert instantiation for a round (payloads, 4-byte entries,
+    // ranked claims), with its dynamic shared-memory limit raised.
+    template <bool RANKED>
+    static cudaError_t seg_insert_kernel(bool payload, bool narrow, int smem, SegKernel* k) {
+        cudaError_t e = cudaSuccess;
+        if (payload && narrow) {
+            e = ensure_smem_attr<k_seg_insert<C, true, true, RANKED>>(smem);
+            *k = k_seg_insert<C, true, true, RANKED>;
+        } else if (payload) {
+            e = ensure_smem_attr<k_seg_insert<C, true, false, RANKED>>(smem);
+            *k = k_seg_insert<C, true, false, RANKED>;
+        } else if (narrow) {
+            e = ensure_smem_attr<k_seg_insert<C, false, true, RANKED>>(smem);
+            *k = k_seg_insert<C, false, true, RANKED>;
+        } else {
+            e = ensure_smem_attr<k_seg_insert<C, false, false, RANKED>>(smem);
+            *k = k_seg_insert<C, false, false, RANKED>;
+        }
+        return e;
+    }
+
+    // ranked: inserts of a batch of at least one key per bucket claim slots
+    // by arrival rank (buckets of at most 16 slots; see k_seg_insert).
     template <int OP>
     static cudaError_t seg_round(const DevTable& t, const SegGeom& g, const SegWork& w, int buf, bool payload,
                                  int round, uint64_t n, bool have_start, bool narrow, cudaStream_t s,
-                                 uint32_t cap = C::bs, int fwd_other = -1) {
+                                 uint32_t cap = C::bs, int fwd_other = -1, bool ranked = false) {
         if (fwd_other < 0) fwd_other = round == 1 ? 1 : 0;
         // inserts claim slots on a per-bucket mask of at most 64 bits, staged
         // beside the segment; buckets of more slots insert with
         // compare-and-swap on the staged words
         constexpr bool masked = OP == SEG_INSERT && C::bs <= 64;
+        constexpr bool rankable = masked && C::bs <= 16;
         constexpr int kMaxSmem = masked ? kSegBytes + (kSegBytes / C::bucket_bytes) * sizeof(SlotMask<C>) : kSegBytes;
-        constexpr auto kern = [] {
-            if constexpr (masked) return k_seg_insert<C, false>;
-            else return k_seg<C, OP>;
-        }();
-        constexpr auto kern_pay = [] {
-            if constexpr (masked) return k_seg_insert<C, true>;
-            else return k_seg<C, OP>;
-        }();
         const int smem = static_cast<int>(masked ? seg_insert_smem<C>(g.sb_log2)
                                                  : (1ull << g.sb_log2) * C::bucket_bytes);
-        cudaError_t e = ensure_smem_attr<kern>(kMaxSmem);
-        if (e == cudaSuccess) e = ensure_smem_attr<kern_pay>(kMaxSmem);
+        SegKernel kern = nullptr;
+        cudaError_t e = cudaSuccess;
+        if constexpr (!masked) {
+            e = ensure_smem_attr<k_seg<C, OP>>(kMaxSmem);
+            kern = k_seg<C, OP>;
+        } else if constexpr (rankable) {
+            e = ranked ? seg_insert_kernel<true>(payload, narrow, kMaxSmem, &kern)
+                       : seg_insert_kernel<false>(payload, narrow, kMaxSmem, &kern);
+        } else {
+            e = seg_insert_kernel<false>(payload, narrow, kMaxSmem, &kern);
+        }
         if (e != cudaSuccess) return e;
         if (!have_start) {
             const uint64_t bthreads = n / 8 + 1;  // 8 positions per thread
@@ -340,12 +369,10 @@ struct Launchers {
         // striding over the segments)
         const int grid = static_cast<int>(g.nseg < 0x7FFFFFFFull ? g.nseg : 0x7FFFFFFFull);
         const int threads = masked ? kSegInsertThreads : kSegThreads;
-        { (payload ? kern_pay : kern)<<<grid, threads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr,
-                                                                     w.start, g.nseg, g.sb_log2, round, w.ent[other],
-                                                                     payload ? w.pay[other] : nullptr,
-                                                                     &w.cnt[round == 3 ? 3 : round - 1],
-                                                                     payload ? w.bitmap : nullptr, narrow ? 1 : 0, cap,
-                                                                     fwd_other); CF_COUNT_LAUNCH(); }
+        { kern<<<grid, threads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start, g.nseg, g.sb_log2,
+                                          round, w.ent[other], payload ? w.pay[other] : nullptr,
+                                          &w.cnt[round == 3 ? 3 : round - 1], payload ? w.bitmap : nullptr,
+                                          narrow ? 1 : 0, cap, fwd_other); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
 
@@ -368,8 +395,10 @@ struct Launchers {
                               : m >= t.nb_mask + 1           ? round1_cap()
                                                              : C::bs;
         const bool round3 = cap1 < C::bs;
+        // batches of at least one key per bucket: slot order within a bucket is unspecified
+        const bool ranked = OP == SEG_INSERT && m >= t.nb_mask + 1;
         if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a, &have_start, &narrow);
-        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, narrow, s, cap1, 1);
+        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, narrow, s, cap1, 1, ranked);
         // round 2: keys that missed their primary bucket, now in ent/pay[1 - a]
         if (e == cudaSuccess) e = cudaMemcpyAsync(w.h_cnt, w.cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -381,7 +410,7 @@ struct Launchers {
                 int c = b;
                 e = sort_by_segment(false, payload, t, g, w, nullptr, b, m2, s, &c, &have_start, &narrow);
                 if (e == cudaSuccess) e = seg_round<OP>(t, g, w, c, payload, 2, m2, have_start, narrow, s, C::bs,
-                                                        round3 ? 1 : 0);
+                                                        round3 ? 1 : 0, ranked);
                 unsigned long long* left = &w.cnt[1];  // keys for eviction: ent/pay[1 - c], count *left
                 bool evict = true;
                 if (e == cudaSuccess && OP == SEG_INSERT && round3) {
@@ -394,7 +423,7 @@ struct Launchers {
                         int c3 = 1 - c;
                         e = sort_by_segment(false, payload, t, g, w, nullptr, 1 - c, m3, s, &c3, &have_start, &narrow);
                         if (e == cudaSuccess) e = seg_round<OP>(t, g, w, c3, payload, 3, m3, have_start, narrow, s,
-                                                                C::bs, 1);
+                                                                C::bs, 1, ranked);
                         c = c3;
                         left = &w.cnt[3];
                     }
@@ -407,7 +436,7 @@ struct Launchers {
                         { k_evict_bfs_steps<C><<<w.sms * bfs_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[1 - c],
                                                                            payload ? w.pay[1 - c] : nullptr,
                                                                            left, bm, w.ent[c],
-                                                                           payload ? w.pay[c] : nullptr, &w.cnt[2]); CF_COUNT_LAUNCH(); }
+                                                                           payload ? w.pay[c] : nullptr, &w.cnt[2], 1u); CF_COUNT_LAUNCH(); }
                         { k_evict_list<C><<<w.sms * list_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[c], payload ? w.pay[c] : nullptr,
                                                                         &w.cnt[2], 0u, max_ev, bm, 1u); CF_COUNT_LAUNCH(); }
                     } else {
@@ -507,7 +536,7 @@ struct Launchers {
                 static const int list_bps = blocks_per_sm(k_evict_list<C>, 256, 0);
                 if (policy_bfs) {
                     { k_evict_bfs_steps<C><<<w.sms * bfs_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], bm, w.ent[0], p0,
-                                                                       &w.cnt[2]); CF_COUNT_LAUNCH(); }
+                                                                       &w.cnt[2], 1u); CF_COUNT_LAUNCH(); }
                     { k_evict_list<C><<<w.sms * list_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[0], p0, &w.cnt[2], 0u, max_ev, bm, 1u); CF_COUNT_LAUNCH(); }
                 } else {
                     { k_evict_list<C><<<w.sms * list_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[1], p1, &w.cnt[1], 0u, max_ev, bm, 0u); CF_COUNT_LAUNCH(); }

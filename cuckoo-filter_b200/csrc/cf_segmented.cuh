@@ -66,17 +66,22 @@ __device__ __forceinline__ uint64_t pack_entry(uint64_t bucket, uint32_t fp) {
 }
 
 template <class C>
-__device__ __forceinline__ uint64_t key_entry(const void* keys, uint64_t i, uint64_t nb_mask) {
-    uint64_t key;
+__device__ __forceinline__ uint64_t load_key(const void* keys, uint64_t i) {
     if constexpr (C::key_bytes == 8)
-        key = ld_stream_u64(static_cast<const uint64_t*>(keys) + i);
+        return ld_stream_u64(static_cast<const uint64_t*>(keys) + i);
     else
-        key = ld_stream_u32(static_cast<const uint32_t*>(keys) + i);
+        return ld_stream_u32(static_cast<const uint32_t*>(keys) + i);
+}
+
+// Packed (primary bucket, tag) entry of a key.
+template <class C>
+__device__ __forceinline__ uint64_t entry_of_key(uint64_t key, uint64_t nb_mask) {
     uint64_t b;
     uint32_t fp;
     candidates<C>(key, nb_mask, b, fp);
     return pack_entry<C>(b, fp);
 }
+
 
 // Number of items of a radix pass: fixed, or read from a device counter.
 __device__ __forceinline__ uint64_t item_count(uint64_t n, const unsigned long long* n_dev) {
@@ -145,12 +150,17 @@ __global__ void __launch_bounds__(kRsHistThreads, 3)
             }
             straddle = lf != ll;
         }
+        // every load of the step is issued before any key is hashed
         uint64_t e[U];
 #pragma unroll
         for (int j = 0; j < U; ++j) {
             const uint64_t i = b + static_cast<uint64_t>(j) * blockDim.x + threadIdx.x;
             e[j] = 0;
-            if (i < hi) e[j] = KEYS ? key_entry<C>(src, i, nb_mask) : ent[i];
+            if (i < hi) e[j] = KEYS ? load_key<C>(src, i) : ent[i];
+        }
+        if constexpr (KEYS) {
+#pragma unroll
+            for (int j = 0; j < U; ++j) e[j] = entry_of_key<C>(e[j], nb_mask);
         }
 #pragma unroll
         for (int j = 0; j < U; ++j) {
@@ -646,11 +656,13 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
 // returned, as tryInsertAtBucket does.  A lane whose key is done takes the
 // next key of its warp's share of the list.  Keys whose candidates all fail go
 // to `dfs` for the DFS fallback.
+// count_keys: add the keys to the evicting-insert counter (0 when an earlier
+// eviction kernel counted them already).
 template <class C>
 __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_steps(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                          const unsigned long long* n_dev, uint32_t* bitmap,
                                                          uint64_t* dfs, uint32_t* dfs_pay,
-                                                         unsigned long long* dfs_count) {
+                                                         unsigned long long* dfs_count, uint32_t count_keys) {
     constexpr uint32_t NC = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
     constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
     // phase = the operation in flight
@@ -824,6 +836,118 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
     }
     flush_counter(&t.ctr[CTR_OCCUPIED], n_ok + n_dup);
     flush_counter(&t.ctr[CTR_DUP], n_dup);
+    flush_counter(&t.ctr[CTR_EVICTED_INSERTS], count_keys ? n_evk : 0u);
+    flush_counter(&t.ctr[CTR_EVICTIONS], n_ev);
+    if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
+// Candidates each key probes at once in the fast eviction pass.
+constexpr int kBfsFastProbes = 2;
+
+// Fast first pass of BFS eviction for a list of keys whose two buckets were
+// full (entries carry (alternate bucket, tag)).  Every lane runs the same
+// fixed sequence, so a warp stays converged: load the entry, snapshot the
+// start bucket (i1 for an even tag, i2 for an odd one), load the alternate
+// buckets of the first P candidates of the reference's order (slots
+// (fp + 7i) & (bs-1), CuckooFilter.cuh:967-1018) all at once, then take the
+// first candidate in that order that can move: an empty candidate slot ->
+// insert fp into the start bucket; else copy the candidate into its
+// alternate bucket and swap fp into its slot if the slot still holds it
+// (undoing the copy otherwise).  A key whose first P candidates cannot move,
+// or whose compare-and-swap finds a bucket changed, goes to `rest`, where the
+// step-machine BFS starts it over.  One key alone takes the reference's steps.
+template <class C, int P>
+__global__ void __launch_bounds__(256) k_evict_bfs_fast(DevTable t, const uint64_t* ent, const uint32_t* pay,
+                                                        const unsigned long long* n_dev, uint32_t* bitmap,
+                                                        uint64_t* rest, uint32_t* rest_pay,
+                                                        unsigned long long* rest_count) {
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    constexpr int NC = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
+    // wide buckets keep one alternate image in registers
+    constexpr int NP = C::nchunks > 4 ? 1 : (P < NC ? P : NC);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint64_t m = *n_dev;
+    uint32_t n_evk = 0, n_ok = 0, n_ev = 0, n_dup = 0;
+    bool err = false;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    // warp-uniform trip count: every lane reaches the ballot below
+    for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x; base < m; base += stride) {
+        const uint64_t i = base + threadIdx.x;
+        const bool v = i < m;
+        bool done = false;
+        uint64_t e = 0;
+        if (v) {
+            ++n_evk;
+            e = __ldcs(reinterpret_cast<const unsigned long long*>(ent) + i);
+            const uint32_t fp0 = static_cast<uint32_t>(e) & C::tag_mask;
+            const uint64_t i2 = e >> C::bits;
+            const uint64_t i1 = alt_bucket<C>(i2, fp0, t.nb_mask);
+            const uint64_t start = (fp0 & 1u) == 0 ? i1 : i2;
+            const uint32_t fp = (fp0 & 1u) == 0 ? alt_tag<C>(fp0) : fp0;  // the tag in the start bucket's form
+            uint64_t* sbw = bucket_words<C>(t, start);
+            uint64_t snap[C::nchunks];
+            load_rlx<C::bucket_bytes>(sbw, snap);
+            uint32_t cand[NP];
+            uint64_t ab[NP];
+            int sw[NP], sh[NP];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * q) & (C::bs - 1));
+                sw[q] = static_cast<int>(slot / C::lanes_per_chunk);
+                sh[q] = static_cast<int>(slot % C::lanes_per_chunk) * C::bits;
+                cand[q] = static_cast<uint32_t>((pick(snap, sw[q]) >> sh[q]) & lane_mask);
+                ab[q] = cand[q] ? alt_bucket<C>(start, cand[q], t.nb_mask) : start;
+            }
+            uint64_t img[NP][C::nchunks];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) load_rlx<C::bucket_bytes>(bucket_words<C>(t, ab[q]), img[q]);
+            bool stop = false;
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                if (stop) continue;
+                if (cand[q] == 0) {  // reference :980-985: the slot is free, insert fp into the start bucket
+                    done = try_insert<C>(sbw, snap, fp, err);
+                    if (done) record_chain(t, 0u);
+                    stop = true;
+                    continue;
+                }
+                int w;
+                uint64_t exp, des;
+                if (!plan_insert<C>(img[q], alt_tag<C>(cand[q]), w, exp, des)) continue;  // no room: next candidate
+                stop = true;
+                if (cas64(bucket_words<C>(t, ab[q]) + w, exp, des) != exp) continue;  // bucket changed: start over later
+                const uint64_t word = pick(snap, sw[q]);
+                const uint64_t swapped = (word & ~(lane_mask << sh[q])) | (static_cast<uint64_t>(fp) << sh[q]);
+                if (cas64(sbw + sw[q], word, swapped) == word) {
+                    done = true;
+                    ++n_ev;
+                    record_chain(t, 1u);
+                } else if (!remove_from_pair<C>(t, ab[q], start, alt_tag<C>(cand[q]), err)) {
+                    ++n_dup;  // the copy could not be taken back: an extra entry
+                }
+            }
+            if (done) {
+                ++n_ok;
+                if (bitmap) atomicOr(&bitmap[pay[i] >> 5], 1u << (pay[i] & 31));
+            }
+        }
+        const bool to_rest = v && !done;
+        const uint32_t push = __ballot_sync(0xFFFFFFFFu, to_rest);
+        if (push) {
+            unsigned long long o = 0;
+            if (lane == static_cast<uint32_t>(__ffs(push) - 1))
+                o = atomicAdd(rest_count, static_cast<unsigned long long>(__popc(push)));
+            o = __shfl_sync(0xFFFFFFFFu, o, __ffs(push) - 1);
+            if (to_rest) {
+                const uint64_t at = o + __popc(push & lt_mask);
+                rest[at] = e;
+                if (rest_pay) rest_pay[at] = pay[i];
+            }
+        }
+    }
+    flush_counter(&t.ctr[CTR_OCCUPIED], n_ok + n_dup);
+    flush_counter(&t.ctr[CTR_DUP], n_dup);
     flush_counter(&t.ctr[CTR_EVICTED_INSERTS], n_evk);
     flush_counter(&t.ctr[CTR_EVICTIONS], n_ev);
     if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
@@ -910,27 +1034,76 @@ __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
     return m;
 }
 
-// Segment-staged insert.  The staged segment carries an empty-slot mask per
-// bucket.  A tag takes the first empty slot circularly from slot
+// The slots a round capped at `cap` tags per bucket may claim in a bucket
+// whose empty slots are `m`: the lowest-numbered cap - (tags present) of
+// them (all of them when cap >= bs).
+template <class C>
+__device__ __forceinline__ SlotMask<C> claimable_slots(SlotMask<C> m, uint32_t cap) {
+    if (cap >= static_cast<uint32_t>(C::bs)) return m;
+    const uint32_t present = C::bs - popc_mask(m);
+    uint32_t quota = cap > present ? cap - present : 0u;
+    SlotMask<C> r = 0;
+    for (; m && quota; --quota) {
+        const SlotMask<C> low = m & (~m + 1);
+        r |= low;
+        m ^= low;
+    }
+    return r;
+}
+
+// Position of the r-th set bit (r counted from 0) of a 16-bit mask that has
+// more than r set bits: a binary search over the popcounts of its halves.
+__device__ __forceinline__ uint32_t nth_set_bit16(uint32_t m, uint32_t r) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (int w = 8; w >= 1; w >>= 1) {
+        const uint32_t c = __popc(m & ((1u << w) - 1u));
+        const bool up = r >= c;
+        r = up ? r - c : r;
+        m = up ? m >> w : m;
+        pos += up ? static_cast<uint32_t>(w) : 0u;
+    }
+    return pos;
+}
+
+// Keys per ranked claim batch: the claim words' 16-bit arrival counters are
+// rebuilt from the staged segment after at most this many of a segment's keys,
+// so no counter can wrap.
+constexpr uint32_t kRankBatch = 32768;
+
+// Segment-staged insert.  The staged segment carries one claim word per
+// bucket, and a key whose bucket has room stores its tag there with a plain
+// shared-memory store into the slot its claim gave it; a key whose bucket has
+// no room goes to `next`, keyed by the key's other bucket when fwd_other is
+// set, else unchanged (for eviction).
+//
+// ORDERED claims (RANKED false): the claim word is the mask of claimable
+// slots, and a tag takes the first claimable slot circularly from slot
 // align_down(fp & (bs-1), tagsPerWord) -- exactly the order in which the
-// reference's tryInsertAtBucket scans words and lanes (CuckooFilter.cuh:859-904)
-// -- claimed with one atomic AND on the mask, then written into the slot
-// with a plain store (the claim makes the slot the thread's own).  Tags whose
-// bucket is full go to `next`, keyed by the key's other bucket when
-// fwd_other is set, else unchanged (for eviction).
-// cap: a claim succeeds only while the bucket holds fewer than `cap` tags
-// (C::bs: no limit).  A claim that finds `cap` tags already there gives its
-// slot back, so at most `cap` claims succeed per bucket; a racing claim may
-// see the returned slot as taken and forward its tag, which is always allowed.
+// reference's tryInsertAtBucket scans words and lanes (CuckooFilter.cuh:
+// 859-904) -- claimed with one atomic AND (only a claim of the same slot can
+// fail and retry).  One key alone so takes the reference's slot.
+//
+// RANKED claims (batches of at least one key per bucket, whose slot order
+// within a bucket is unspecified; buckets of at most 16 slots): the claim word
+// holds the 16-bit claimable mask and, above it, a 16-bit arrival counter.
+// One atomic add per key returns both: the key with arrival rank r takes the
+// r-th claimable slot if there is one.  No claim fails or retries.
+//
+// cap: at most `cap` tags per bucket after the round (C::bs: no limit): only
+// the lowest cap - (tags present) empty slots are claimable.  Capped rounds
+// run only for batches of at least one key per bucket.
 // PAY: entries carry payloads (key positions; `pay`, `next_pay` and `bitmap`
-// are used only then).
-template <class C, bool PAY>
+// are used only then).  NARROW: entries are 4-byte ((bucket within the
+// segment) << bits | tag), else 8-byte (bucket << bits | tag).
+template <class C, bool PAY, bool NARROW, bool RANKED>
 __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                             const uint32_t* start, uint64_t nseg, int sb_log2,
                                                             int round, uint64_t* next, uint32_t* next_pay,
                                                             unsigned long long* next_count, uint32_t* bitmap,
-                                                            int narrow, uint32_t cap, int fwd_other) {
+                                                            int /*narrow*/, uint32_t cap, int fwd_other) {
     using M = SlotMask<C>;
+    static_assert(!RANKED || C::bs <= 16, "ranked claims keep a 16-bit counter above a 16-slot mask");
     extern __shared__ __align__(16) uint64_t seg[];
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_base;
@@ -970,12 +1143,28 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
             for (uint32_t w = tid; w < words; w += blockDim.x) seg[w] = gseg[w];
         }
         __syncthreads();
-        for (uint32_t b = tid; b < sb; b += blockDim.x)
-            mask[b] = b < nbk ? empty_mask<C>(seg + static_cast<uint64_t>(b) * WPB) : static_cast<M>(0);
+        // claim words from the staged segment (ranked: counters at zero)
+        auto build_claims = [&]() {
+            for (uint32_t b = tid; b < sb; b += blockDim.x)
+                mask[b] = b < nbk ? claimable_slots<C>(empty_mask<C>(seg + static_cast<uint64_t>(b) * WPB), cap)
+                                  : static_cast<M>(0);
+        };
+        build_claims();
         __syncthreads();
-        constexpr int U = 8;
+        // entries per thread per step: 4-byte entries without payloads stay
+        // 32-bit in registers, so twice as many fit (half the block barriers)
+        constexpr int U = NARROW && !PAY ? 16 : 8;
+        using E = typename std::conditional<NARROW, uint32_t, uint64_t>::type;
         for (uint32_t base = lo; base < hi; base += blockDim.x * U) {
-            uint64_t ev[U];
+            if constexpr (RANKED) {
+                static_assert(kRankBatch % (kSegInsertThreads * U) == 0, "claim batches hold whole steps");
+                if (base != lo && (base - lo) % kRankBatch == 0) {
+                    // the previous step ended with a barrier: every tag is in the staged segment
+                    build_claims();
+                    __syncthreads();
+                }
+            }
+            E ev[U];
             uint32_t pv[PAY ? U : 1];
 #pragma unroll
             for (int j = 0; j < U; ++j) {
@@ -983,7 +1172,10 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                 ev[j] = 0;
                 if constexpr (PAY) pv[j] = 0;
                 if (k < hi) {
-                    ev[j] = narrow ? reinterpret_cast<const uint32_t*>(ent)[k] : ent[k];
+                    if constexpr (NARROW)
+                        ev[j] = reinterpret_cast<const uint32_t*>(ent)[k];
+                    else
+                        ev[j] = ent[k];
                     if constexpr (PAY) pv[j] = pay[k];
                 }
             }
@@ -993,41 +1185,47 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                 const uint32_t k = base + j * blockDim.x + tid;
                 if (k >= hi) continue;
                 const uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
-                const uint32_t lb = static_cast<uint32_t>(ev[j] >> C::bits) & (sb - 1);
-                const uint32_t s0 = ((fp & (C::bs - 1)) / C::tpw) * C::tpw;
-                M m = mask[lb];
+                const uint32_t lb = static_cast<uint32_t>(static_cast<uint64_t>(ev[j]) >> C::bits) & (sb - 1);
                 bool ok = false;
-                for (int it = 0; it < 64 && m; ++it) {
-                    if (C::bs - popc_mask(m) >= cap) break;  // `cap` tags there already
-                    // first empty slot circularly from s0
-                    const M rot = s0 ? (((m >> s0) | (m << (C::bs - s0))) & kFull) : m;
-                    uint32_t off;
-                    if constexpr (sizeof(M) == 8)
-                        off = __ffsll(static_cast<long long>(rot)) - 1;
-                    else
-                        off = __ffs(static_cast<int>(rot)) - 1;
-                    const uint32_t slot = (s0 + off) & (C::bs - 1);
-                    // claim the slot alone: only a claim of the same slot can fail
-                    const M bit = static_cast<M>(1) << slot;
-                    const M old = atomicAnd(&mask[lb], ~bit);
-                    if ((old & bit) && C::bs - popc_mask(old) >= cap) {  // claimed past the cap: give it back
-                        atomicOr(&mask[lb], bit);
-                        break;
-                    }
-                    if (old & bit) {
-                        uint8_t* dst = seg_bytes + (static_cast<uint64_t>(lb) * C::bucket_bytes + slot * TB);
-                        if constexpr (TB == 1)
-                            *dst = static_cast<uint8_t>(fp);
-                        else if constexpr (TB == 2)
-                            *reinterpret_cast<uint16_t*>(dst) = static_cast<uint16_t>(fp);
-                        else
-                            *reinterpret_cast<uint32_t*>(dst) = fp;
+                uint32_t slot = 0;
+                if constexpr (RANKED) {
+                    const uint32_t old = atomicAdd(reinterpret_cast<uint32_t*>(&mask[lb]), 1u << 16);
+                    const uint32_t m = old & 0xFFFFu;
+                    const uint32_t r = old >> 16;
+                    if (r < static_cast<uint32_t>(__popc(m))) {
+                        slot = nth_set_bit16(m, r);
                         ok = true;
-                        break;
                     }
-                    m = old;
+                } else {
+                    const uint32_t s0 = ((fp & (C::bs - 1)) / C::tpw) * C::tpw;
+                    M m = mask[lb];
+                    for (int it = 0; it < 64 && m; ++it) {
+                        // first claimable slot circularly from s0
+                        const M rot = s0 ? (((m >> s0) | (m << (C::bs - s0))) & kFull) : m;
+                        uint32_t off;
+                        if constexpr (sizeof(M) == 8)
+                            off = __ffsll(static_cast<long long>(rot)) - 1;
+                        else
+                            off = __ffs(static_cast<int>(rot)) - 1;
+                        slot = (s0 + off) & (C::bs - 1);
+                        // claim the slot alone: only a claim of the same slot can fail
+                        const M bit = static_cast<M>(1) << slot;
+                        const M old = atomicAnd(&mask[lb], ~bit);
+                        if (old & bit) {
+                            ok = true;
+                            break;
+                        }
+                        m = old;
+                    }
                 }
                 if (ok) {
+                    uint8_t* dst = seg_bytes + (static_cast<uint64_t>(lb) * C::bucket_bytes + slot * TB);
+                    if constexpr (TB == 1)
+                        *dst = static_cast<uint8_t>(fp);
+                    else if constexpr (TB == 2)
+                        *reinterpret_cast<uint16_t*>(dst) = static_cast<uint16_t>(fp);
+                    else
+                        *reinterpret_cast<uint32_t*>(dst) = fp;
                     ++n_ok;
                     if constexpr (PAY) atomicOr(&bitmap[pv[j] >> 5], 1u << (pv[j] & 31));
                 } else {
@@ -1053,7 +1251,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                     if ((fwd_mask >> j) & 1u) {
                         const uint32_t fp = static_cast<uint32_t>(ev[j]) & C::tag_mask;
                         // the full bucket index from the segment (entries may be 4-byte)
-                        uint64_t b = (s << sb_log2) | ((ev[j] >> C::bits) & (sb - 1));
+                        uint64_t b = (s << sb_log2) | ((static_cast<uint64_t>(ev[j]) >> C::bits) & (sb - 1));
                         uint32_t tg = fp;
                         if (fwd_other) {  // keyed by the other bucket, the tag in that bucket's form
                             b = alt_bucket<C>(b, fp, t.nb_mask);

@@ -143,10 +143,10 @@ def test_workspace_default_is_automatic_and_holds_the_whole_batch(cfb, orc):
     """The default workspace limit is automatic: a batch that fits the free
     device memory runs in one chunk (16 bytes per key without per-key results,
     about 24 with them), and the workspace is kept for later calls."""
-    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 24)
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 25)
     try:
         assert f.getOption(cfb.OPT_WORKSPACE_LIMIT) == 0
-        n = 1 << 23
+        n = 1 << 23  # two batches fill the table to half its capacity
         keys = orc.splitmix64(91, n)
         occ = f.insertManySorted(dev(keys))
         ws = f.getOption(cfb.OPT_WORKSPACE_BYTES)
