@@ -582,6 +582,9 @@ def run_b200(args, w: dict) -> dict | None:
     f = cfb.CuckooFilter(cfg, w["capacity"])
     if args.workspace_gb is not None:
         f.setOption(cfb.OPT_WORKSPACE_LIMIT, int(args.workspace_gb * (1 << 30)))
+    staging = {"auto": cfb.STAGING_AUTO, "random": cfb.STAGING_RANDOM, "segment": cfb.STAGING_SEGMENT,
+               "region": cfb.STAGING_REGION}[args.staging]
+    f.setOption(cfb.OPT_STAGING, staging)
     fill, query, dele, n_coll, is_pos = make_inputs(w, dev, rank, with_mask=True)
     n_fill, n_q, n_d = fill.numel(), query.numel(), dele.numel()
     q_out = torch.empty(n_q, dtype=torch.bool, device=dev)
@@ -671,15 +674,23 @@ def run_b200(args, w: dict) -> dict | None:
         return {"gkeys_s": n / t / 1e9, "ms": statistics.mean(ms), "algorithmic_bytes": b,
                 "achieved_gbs": b / t / 1e9, "frac_of_hbm": b / t / 1e9 / peak}
 
-    ops = {"insert": op(n_fill, ins_ms, ins_bytes), "contains": op(n_q, con_ms, con_bytes),
-           "delete": op(n_d, del_ms, del_bytes), "clear_ms": statistics.mean(
+    ops = {"insert": {**op(n_fill, ins_ms, ins_bytes), "ms_steps": ins_ms},
+           "contains": {**op(n_q, con_ms, con_bytes), "ms_steps": con_ms},
+           "delete": {**op(n_d, del_ms, del_bytes), "ms_steps": del_ms}, "clear_ms": statistics.mean(
                [evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)])}
-    ops["insert"]["path"] = "insertManySorted (segment-staged)" if sorted_fill else "insertMany (random CAS)"
-    # the library's automatic choice (CF_OPT_SEGMENTED_MIN_KEYS = 0): segment path from 8 keys per bucket
-    seg_q = n_q >= f.getNumBuckets() * 8
-    seg_d = n_d >= f.getNumBuckets() * 8
-    ops["contains"]["path"] = "segment-staged" if seg_q else "random probes"
-    ops["delete"]["path"] = "segment-staged" if seg_d else "random probes"
+    # the library's automatic choice (CF_OPT_SEGMENTED_MIN_KEYS = 0): inserts are
+    # segment-staged from one key per bucket, lookups and deletes from eight
+    def path_of(n, per_bucket):
+        if args.staging != "auto":
+            return {"random": "random probes", "segment": "segment-staged", "region": "region-staged"}[args.staging]
+        return "segment-staged" if n >= f.getNumBuckets() * per_bucket else "random probes"
+
+    ins_path = path_of(n_fill, 1)
+    ops["insert"]["path"] = ("insertManySorted (segment-staged)" if sorted_fill and args.staging != "region" else
+                             "insertManySorted (region-staged)" if sorted_fill else
+                             "insertMany (random CAS)" if ins_path == "random probes" else f"insertMany ({ins_path})")
+    ops["contains"]["path"] = path_of(n_q, 8)
+    ops["delete"]["path"] = path_of(n_d, 8)
 
     # plain insertMany on the random CAS path (a fill this large would be
     # segment-staged by default), on the same fill, timed on its own
@@ -699,7 +710,7 @@ def run_b200(args, w: dict) -> dict | None:
         ops["insert_plain"] = op(n_fill, ts, n_fill * 72 + 32 * (st_p["secondary"] + st_p["evicted_inserts"]))
         ops["insert_plain"]["path"] = "insertMany (random CAS), not part of the step"
         ops["insert_plain"]["failed"] = st_p["failed"]
-        f.setOption(cfb.OPT_STAGING, cfb.STAGING_AUTO)
+        f.setOption(cfb.OPT_STAGING, staging)
     for name in ("insert", "contains", "delete"):
         tr = load_traffic(name, w, ops[name]["path"])
         if tr:
@@ -1950,6 +1961,10 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large")
+    ap.add_argument("--bits", type=int, choices=(8, 16, 32), default=None,
+                    help="override the workload's bits per tag (plain form; 32-bit tags use 8-slot buckets)")
+    ap.add_argument("--staging", choices=("auto", "random", "segment", "region"), default="auto",
+                    help="plain form: force every batch onto one execution path (CF_OPT_STAGING)")
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--insert", choices=("auto", "plain", "sorted"), default="auto",
                     help="fill with insertMany (plain), insertManySorted (sorted), or as the reference's benchmark "
@@ -1994,7 +2009,10 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 1:
         ap.error("--warmup must be >= 1")
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.bits:
+        w["bits"], w["bs"] = args.bits, 8 if args.bits == 32 else 16
+        w["desc"] += f" [bits per tag {w['bits']}, bucket size {w['bs']}]"
     if args.form == "batched":
         res = run_batched(args)
     elif args.form == "served":

@@ -225,15 +225,25 @@ void init_geometry(cf_filter* f) {
     f->rgeom.nreg = static_cast<uint32_t>(((f->num_buckets - 1) >> rl) + 1);
 }
 
+// Words of the known-full bucket bitmap (one bit per bucket of the segment
+// geometry), kept when the segment insert runs k_seg_insert (at most 64
+// slots per bucket) on segments of at least 32 buckets; else 0.
+uint64_t full_words(const cf_filter* f) {
+    if (f->cfg.bucket_size > 64 || f->geom.sb_log2 < 5) return 0;
+    return (f->geom.nseg << f->geom.sb_log2) >> 5;
+}
+
 // Bytes of workspace for a chunk of `cap` keys: two entry buffers (8 B per
-// key), and with per-key results two payload buffers (4 B) and a result bitmap.
+// key), and with per-key results two payload buffers (4 B) and a result bitmap;
+// besides, per table, the radix histogram, the segment starts, the list
+// counters and the known-full bucket bitmap.
 uint64_t ws_need(const cf_filter* f, uint64_t cap, int grid, bool payload) {
     const uint64_t hist = static_cast<uint64_t>(kRadix) * grid * 4;
     const uint64_t start = (f->geom.nseg + 1) * 4;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     // result bitmap: two bits per key (a region-staged lookup keeps one hit bit per staged entry)
     const uint64_t per_key = payload ? al(cap * 4) * 2 + al((2 * cap + 31) / 32 * 4) : 0;
-    return al(cap * 8) * 2 + per_key + al(hist) + al(start) + al(64);
+    return al(cap * 8) * 2 + per_key + al(hist) + al(start) + al(64) + al(full_words(f) * 4);
 }
 
 // Automatic workspace limit (CF_OPT_WORKSPACE_LIMIT = 0, the default): the
@@ -313,6 +323,9 @@ int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     p += al((f->geom.nseg + 1) * 4);
     w->cnt = reinterpret_cast<unsigned long long*>(p);
     p += al(64);
+    w->full_words = full_words(f);
+    w->full = w->full_words ? reinterpret_cast<uint32_t*>(p) : nullptr;
+    p += al(w->full_words * 4);
     w->pay[0] = w->pay[1] = nullptr;
     w->bitmap = nullptr;
     if (payload) {
@@ -992,6 +1005,8 @@ int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8
     w.start = reinterpret_cast<uint32_t*>(p);
     p += kNaStart;
     w.cnt = reinterpret_cast<unsigned long long*>(p);
+    w.full = nullptr;  // no known-full bitmap in the fixed scratch: eviction probes every candidate
+    w.full_words = 0;
     w.h_cnt = f->h_cnt;
     w.cap = kNoAllocMaxKeys;
     w.sms = f->sms;

@@ -40,9 +40,15 @@ struct SegWork {
     uint32_t* pay[2];
     uint32_t* hist;   // kRadix * max(rs_grid)
     uint32_t* start;  // nseg + 1
-    unsigned long long* cnt;   // [2] list lengths
+    unsigned long long* cnt;   // list lengths (5 used; 8 allocated)
     unsigned long long* h_cnt; // pinned mirror
     uint32_t* bitmap;          // cap / 32 words
+    // Known-full buckets of the table, one bit per bucket (full_words words),
+    // written by the segment insert rounds and read by eviction; null when
+    // not kept (buckets of more than 64 slots, segments of fewer than 32
+    // buckets, or the fixed scratch of cf_insert_sorted_noalloc).
+    uint32_t* full;
+    uint64_t full_words;
     uint64_t cap;
     int rs_grid[3];  // radix CTAs per payload mode (one wave of that scatter kernel)
     int sms;       // streaming multiprocessors
@@ -309,7 +315,7 @@ struct Launchers {
 
     // Every kernel of a segment round has this signature (k_seg and k_seg_insert).
     using SegKernel = void (*)(DevTable, const uint64_t*, const uint32_t*, const uint32_t*, uint64_t, int, int,
-                               uint64_t*, uint32_t*, unsigned long long*, uint32_t*, int, uint32_t, int);
+                               uint64_t*, uint32_t*, unsigned long long*, uint32_t*, int, uint32_t, int, uint32_t*);
 
     // The k_seg_insert instantiation for a round (payloads, 4-byte entries,
     // ranked claims), with its dynamic shared-memory limit raised.
@@ -372,7 +378,8 @@ struct Launchers {
         { kern<<<grid, threads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start, g.nseg, g.sb_log2,
                                           round, w.ent[other], payload ? w.pay[other] : nullptr,
                                           &w.cnt[round == 3 ? 3 : round - 1], payload ? w.bitmap : nullptr,
-                                          narrow ? 1 : 0, cap, fwd_other); CF_COUNT_LAUNCH(); }
+                                          narrow ? 1 : 0, cap, fwd_other, OP == SEG_INSERT ? w.full : nullptr);
+          CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
 
@@ -380,8 +387,12 @@ struct Launchers {
     static cudaError_t seg_chunk_op(const DevTable& t, const SegGeom& g, const SegWork& w, const void* keys,
                                     uint64_t m, uint8_t* out, cudaStream_t s, uint32_t policy_bfs, uint32_t max_ev) {
         const bool payload = out != nullptr;
-        cudaError_t e = cudaMemsetAsync(w.cnt, 0, 4 * sizeof(unsigned long long), s);
+        // list lengths: round-1, round-2, eviction (DFS), round-3 and fast-eviction leftovers
+        cudaError_t e = cudaMemsetAsync(w.cnt, 0, 5 * sizeof(unsigned long long), s);
         if (e == cudaSuccess && payload) e = cudaMemsetAsync(w.bitmap, 0, (m + 31) / 32 * 4, s);
+        // known-full buckets: none known at the start of a batch
+        if (e == cudaSuccess && OP == SEG_INSERT && w.full)
+            e = cudaMemsetAsync(w.full, 0, w.full_words * sizeof(uint32_t), s);
         int a = 0;
         bool have_start = false, narrow = false;
         // Fills of at least one key per bucket: the first round leaves
@@ -433,11 +444,21 @@ struct Launchers {
                     static const int bfs_bps = blocks_per_sm(k_evict_bfs_steps<C>, 256, 0);
                     static const int list_bps = blocks_per_sm(k_evict_list<C>, 256, 0);
                     if (policy_bfs) {
-                        { k_evict_bfs_steps<C><<<w.sms * bfs_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[1 - c],
-                                                                           payload ? w.pay[1 - c] : nullptr,
-                                                                           left, bm, w.ent[c],
-                                                                           payload ? w.pay[c] : nullptr, &w.cnt[2], 1u); CF_COUNT_LAUNCH(); }
-                        { k_evict_list<C><<<w.sms * list_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[c], payload ? w.pay[c] : nullptr,
+                        // a lockstep pass over the first candidates, then the
+                        // step machine for what it could not place, then DFS
+                        static const int fast_bps = blocks_per_sm(k_evict_bfs_fast<C, kBfsFastProbes>, 256, 0);
+                        uint32_t* p_in = payload ? w.pay[1 - c] : nullptr;
+                        uint32_t* p_mid = payload ? w.pay[c] : nullptr;
+                        // keys whose candidates all fail are flagged for DFS when
+                        // entries leave bit 63 free
+                        const int bucket_bits = t.nb_mask ? 64 - __builtin_clzll(t.nb_mask) : 0;
+                        const uint32_t flag_ok = bucket_bits + C::bits <= 63 ? 1u : 0u;
+                        { k_evict_bfs_fast<C, kBfsFastProbes><<<w.sms * fast_bps * kEvictGridWaves, 256, 0, s>>>(
+                              t, w.ent[1 - c], p_in, left, bm, w.ent[c], p_mid, &w.cnt[4], w.full, flag_ok);
+                          CF_COUNT_LAUNCH(); }
+                        { k_evict_bfs_steps<C><<<w.sms * bfs_bps * kEvictGridWaves, 256, 0, s>>>(
+                              t, w.ent[c], p_mid, &w.cnt[4], bm, w.ent[1 - c], p_in, &w.cnt[2], 0u); CF_COUNT_LAUNCH(); }
+                        { k_evict_list<C><<<w.sms * list_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[1 - c], p_in,
                                                                         &w.cnt[2], 0u, max_ev, bm, 1u); CF_COUNT_LAUNCH(); }
                     } else {
                         { k_evict_list<C><<<w.sms * list_bps * kEvictGridWaves, 256, 0, s>>>(t, w.ent[1 - c],

@@ -57,6 +57,9 @@ constexpr int kRsHistThreads = 512;
 constexpr int kRsHistSub = 3;
 static_assert(kRsThreads == kRadix, "the scatter's per-digit phases give one thread per digit");
 constexpr int kSegBytes = 65536;
+// Entry flag (bit 63) for the step-machine BFS: this key's BFS candidates all
+// failed already, send it to DFS.  Used only where entries leave bit 63 free.
+constexpr uint64_t kDfsFlag = 1ull << 63;
 constexpr int kSegThreads = 256;
 constexpr int kSegInsertThreads = 256;
 
@@ -505,7 +508,7 @@ __global__ void __launch_bounds__(kSegThreads) k_seg(DevTable t, const uint64_t*
                                                      const uint32_t* start, uint64_t nseg, int sb_log2, int round,
                                                      uint64_t* next, uint32_t* next_pay,
                                                      unsigned long long* next_count, uint32_t* bitmap, int narrow,
-                                                     uint32_t /*cap*/, int fwd_other) {
+                                                     uint32_t /*cap*/, int fwd_other, uint32_t* /*full*/) {
     extern __shared__ __align__(16) uint64_t seg[];
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_base;
@@ -743,6 +746,11 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
             switch (phase) {
                 case P_FETCH: {
                     e = ld[0];
+                    if (e & kDfsFlag) {  // BFS already failed for this key: straight to DFS
+                        e &= ~kDfsFlag;
+                        outcome = 3;
+                        break;
+                    }
                     fp = static_cast<uint32_t>(e) & C::tag_mask;
                     const uint64_t i2 = e >> C::bits;
                     const uint64_t i1 = alt_bucket<C>(i2, fp, t.nb_mask);
@@ -841,30 +849,45 @@ __global__ void __launch_bounds__(256, C::nchunks <= 4 ? 3 : 2) k_evict_bfs_step
     if (__any_sync(0xFFFFFFFFu, err) && lane == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
 }
 
-// Candidates each key probes at once in the fast eviction pass.
+// Alternate buckets a key may probe in the fast eviction pass before it is
+// left to the step-machine BFS.
 constexpr int kBfsFastProbes = 2;
+__device__ __forceinline__ bool known_full(const uint32_t* full, uint64_t b) {
+    return full && ((full[b >> 5] >> (b & 31)) & 1u);
+}
+
+// Empty slots of a bucket image (zero_lanes flags exactly the empty lanes).
+template <class C>
+__device__ __forceinline__ uint32_t empty_count(const uint64_t (&c)[C::nchunks]) {
+    uint32_t n = 0;
+#pragma unroll
+    for (int j = 0; j < C::nchunks; ++j) n += __popcll(zero_lanes<C::bits>(c[j]));
+    return n;
+}
 
 // Fast first pass of BFS eviction for a list of keys whose two buckets were
 // full (entries carry (alternate bucket, tag)).  Every lane runs the same
-// fixed sequence, so a warp stays converged: load the entry, snapshot the
-// start bucket (i1 for an even tag, i2 for an odd one), load the alternate
-// buckets of the first P candidates of the reference's order (slots
-// (fp + 7i) & (bs-1), CuckooFilter.cuh:967-1018) all at once, then take the
-// first candidate in that order that can move: an empty candidate slot ->
-// insert fp into the start bucket; else copy the candidate into its
-// alternate bucket and swap fp into its slot if the slot still holds it
-// (undoing the copy otherwise).  A key whose first P candidates cannot move,
-// or whose compare-and-swap finds a bucket changed, goes to `rest`, where the
+// short sequence: load the entry, snapshot the start bucket (i1 for an even
+// tag, i2 for an odd one), then take the reference's candidates in order
+// (slots (fp + 7i) & (bs-1), CuckooFilter.cuh:967-1018): an empty candidate
+// slot -> insert fp into the start bucket; a candidate whose alternate bucket
+// is known full (`full`, one bit per bucket, set by the segment rounds and
+// kept up to date here; buckets only fill during an insert) is passed over
+// without a probe, exactly as the reference's probe of it would find no room;
+// otherwise its alternate bucket is loaded, the candidate copied there and fp
+// swapped into its slot if the slot still holds it (the copy is undone
+// otherwise).  A key whose candidates all fail goes to DFS (flagged for the
+// step machine when flag_ok, else through it); a key that used its P probes,
+// or whose compare-and-swap found a bucket changed, goes to `rest`, where the
 // step-machine BFS starts it over.  One key alone takes the reference's steps.
 template <class C, int P>
 __global__ void __launch_bounds__(256) k_evict_bfs_fast(DevTable t, const uint64_t* ent, const uint32_t* pay,
                                                         const unsigned long long* n_dev, uint32_t* bitmap,
                                                         uint64_t* rest, uint32_t* rest_pay,
-                                                        unsigned long long* rest_count) {
+                                                        unsigned long long* rest_count, uint32_t* full,
+                                                        uint32_t flag_ok) {
     constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
     constexpr int NC = (C::bs / 2) < 8 ? (C::bs / 2) : 8;
-    // wide buckets keep one alternate image in registers
-    constexpr int NP = C::nchunks > 4 ? 1 : (P < NC ? P : NC);
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint64_t m = *n_dev;
@@ -875,7 +898,7 @@ __global__ void __launch_bounds__(256) k_evict_bfs_fast(DevTable t, const uint64
     for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x; base < m; base += stride) {
         const uint64_t i = base + threadIdx.x;
         const bool v = i < m;
-        bool done = false;
+        bool done = false, stop = false;
         uint64_t e = 0;
         if (v) {
             ++n_evk;
@@ -888,48 +911,73 @@ __global__ void __launch_bounds__(256) k_evict_bfs_fast(DevTable t, const uint64
             uint64_t* sbw = bucket_words<C>(t, start);
             uint64_t snap[C::nchunks];
             load_rlx<C::bucket_bytes>(sbw, snap);
-            uint32_t cand[NP];
-            uint64_t ab[NP];
-            int sw[NP], sh[NP];
+            uint32_t cand[NC];
+            uint64_t ab[NC];
 #pragma unroll
-            for (int q = 0; q < NP; ++q) {
+            for (int q = 0; q < NC; ++q) {
                 const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * q) & (C::bs - 1));
-                sw[q] = static_cast<int>(slot / C::lanes_per_chunk);
-                sh[q] = static_cast<int>(slot % C::lanes_per_chunk) * C::bits;
-                cand[q] = static_cast<uint32_t>((pick(snap, sw[q]) >> sh[q]) & lane_mask);
+                cand[q] = static_cast<uint32_t>(
+                    (pick(snap, static_cast<int>(slot / C::lanes_per_chunk)) >> ((slot % C::lanes_per_chunk) * C::bits)) &
+                    lane_mask);
                 ab[q] = cand[q] ? alt_bucket<C>(start, cand[q], t.nb_mask) : start;
             }
-            uint64_t img[NP][C::nchunks];
+            // candidates still worth trying: an empty slot, or an alternate
+            // bucket not known to be full (bit q, in the reference's order)
+            uint32_t avail = 0;
 #pragma unroll
-            for (int q = 0; q < NP; ++q) load_rlx<C::bucket_bytes>(bucket_words<C>(t, ab[q]), img[q]);
-            bool stop = false;
+            for (int q = 0; q < NC; ++q)
+                if (cand[q] == 0 || !known_full(full, ab[q])) avail |= 1u << q;
+            // up to P probe rounds; in each, every lane loads its own next
+            // candidate's alternate bucket, so a warp waits one round trip per
+            // round however its lanes' candidates differ
+            for (int r = 0; r < P && !stop && avail; ++r) {
+                const int q = __ffs(avail) - 1;
+                avail &= avail - 1;
+                uint32_t cq = cand[0];
+                uint64_t aq = ab[0];
 #pragma unroll
-            for (int q = 0; q < NP; ++q) {
-                if (stop) continue;
-                if (cand[q] == 0) {  // reference :980-985: the slot is free, insert fp into the start bucket
+                for (int j = 1; j < NC; ++j) {
+                    cq = j == q ? cand[j] : cq;
+                    aq = j == q ? ab[j] : aq;
+                }
+                if (cq == 0) {  // reference :980-985: the slot is free, insert fp into the start bucket
                     done = try_insert<C>(sbw, snap, fp, err);
                     if (done) record_chain(t, 0u);
                     stop = true;
-                    continue;
+                    break;
                 }
+                uint64_t* abw = bucket_words<C>(t, aq);
+                uint64_t img[C::nchunks];
+                load_rlx<C::bucket_bytes>(abw, img);
                 int w;
                 uint64_t exp, des;
-                if (!plan_insert<C>(img[q], alt_tag<C>(cand[q]), w, exp, des)) continue;  // no room: next candidate
+                if (!plan_insert<C>(img, alt_tag<C>(cq), w, exp, des)) {  // no room: remember, next candidate
+                    if (full) atomicOr(&full[aq >> 5], 1u << (aq & 31));
+                    continue;
+                }
                 stop = true;
-                if (cas64(bucket_words<C>(t, ab[q]) + w, exp, des) != exp) continue;  // bucket changed: start over later
-                const uint64_t word = pick(snap, sw[q]);
-                const uint64_t swapped = (word & ~(lane_mask << sh[q])) | (static_cast<uint64_t>(fp) << sh[q]);
-                if (cas64(sbw + sw[q], word, swapped) == word) {
+                if (cas64(abw + w, exp, des) != exp) break;  // the bucket changed: start over later
+                if (full && empty_count<C>(img) == 1) atomicOr(&full[aq >> 5], 1u << (aq & 31));
+                const uint32_t slot = static_cast<uint32_t>((static_cast<uint64_t>(fp) + 7ull * q) & (C::bs - 1));
+                const int sw = static_cast<int>(slot / C::lanes_per_chunk);
+                const int sh = static_cast<int>(slot % C::lanes_per_chunk) * C::bits;
+                const uint64_t word = pick(snap, sw);
+                const uint64_t swapped = (word & ~(lane_mask << sh)) | (static_cast<uint64_t>(fp) << sh);
+                if (cas64(sbw + sw, word, swapped) == word) {
                     done = true;
                     ++n_ev;
                     record_chain(t, 1u);
-                } else if (!remove_from_pair<C>(t, ab[q], start, alt_tag<C>(cand[q]), err)) {
+                } else if (!remove_from_pair<C>(t, aq, start, alt_tag<C>(cq), err)) {
                     ++n_dup;  // the copy could not be taken back: an extra entry
                 }
             }
+            // probes used up with candidates left: the step machine takes the key
+            if (!stop && avail) stop = true;
             if (done) {
                 ++n_ok;
                 if (bitmap) atomicOr(&bitmap[pay[i] >> 5], 1u << (pay[i] & 31));
+            } else if (!stop && flag_ok) {
+                e |= kDfsFlag;  // every candidate failed: BFS is over for this key
             }
         }
         const bool to_rest = v && !done;
@@ -1101,7 +1149,8 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                                                             const uint32_t* start, uint64_t nseg, int sb_log2,
                                                             int round, uint64_t* next, uint32_t* next_pay,
                                                             unsigned long long* next_count, uint32_t* bitmap,
-                                                            int /*narrow*/, uint32_t cap, int fwd_other) {
+                                                            int /*narrow*/, uint32_t cap, int fwd_other,
+                                                            uint32_t* full) {
     using M = SlotMask<C>;
     static_assert(!RANKED || C::bs <= 16, "ranked claims keep a 16-bit counter above a 16-slot mask");
     extern __shared__ __align__(16) uint64_t seg[];
@@ -1264,6 +1313,27 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                 }
             }
             __syncthreads();
+        }
+        if (full && cap >= static_cast<uint32_t>(C::bs)) {
+            // one bit per bucket of the segment, set when an uncapped round
+            // left it without an empty slot, read off its claim word: ranked,
+            // arrivals reached the claimable slots; ordered, no claimable slot
+            // is left.  (A capped round fills no bucket; its bits stay 0,
+            // which only means "not known full".)  sb is a multiple of 32
+            // whenever the bitmap is kept.
+            for (uint32_t b0 = 0; b0 < sb; b0 += blockDim.x) {
+                const uint32_t b = b0 + tid;
+                bool is_full = false;
+                if (b < nbk) {
+                    const M cw = mask[b];
+                    if constexpr (RANKED)
+                        is_full = (static_cast<uint32_t>(cw) >> 16) >= static_cast<uint32_t>(__popc(cw & 0xFFFFu));
+                    else
+                        is_full = cw == 0;
+                }
+                const uint32_t word = __ballot_sync(0xFFFFFFFFu, is_full);
+                if (lane == 0 && b < sb) full[((s << sb_log2) + b) >> 5] = word;
+            }
         }
         if (words % 2 == 0) {
             ulonglong2* g2 = reinterpret_cast<ulonglong2*>(gseg);
