@@ -1242,7 +1242,11 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                     const uint32_t m = old & 0xFFFFu;
                     const uint32_t r = old >> 16;
                     if (r < static_cast<uint32_t>(__popc(m))) {
-                        slot = nth_set_bit16(m, r);
+                        // claimable slots are usually one run of bits (ranks
+                        // fill a bucket in slot order): the r-th is low + r
+                        const uint32_t low = static_cast<uint32_t>(__ffs(m)) - 1u;
+                        const uint32_t run = m >> low;
+                        slot = (run & (run + 1u)) == 0 ? low + r : nth_set_bit16(m, r);
                         ok = true;
                     }
                 } else {
