@@ -1087,7 +1087,10 @@ __device__ __forceinline__ SlotMask<C> empty_mask(const uint64_t* bw) {
 // them (all of them when cap >= bs).
 template <class C>
 __device__ __forceinline__ SlotMask<C> claimable_slots(SlotMask<C> m, uint32_t cap) {
+    using M = SlotMask<C>;
+    constexpr M kAll = C::bs == 8 * sizeof(M) ? ~static_cast<M>(0) : ((static_cast<M>(1) << (C::bs % (8 * sizeof(M)))) - 1);
     if (cap >= static_cast<uint32_t>(C::bs)) return m;
+    if (m == kAll) return (static_cast<M>(1) << cap) - 1;  // an empty bucket: its lowest `cap` slots
     const uint32_t present = C::bs - popc_mask(m);
     uint32_t quota = cap > present ? cap - present : 0u;
     SlotMask<C> r = 0;
@@ -1165,6 +1168,14 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
     M* mask = reinterpret_cast<M*>(seg + seg_words);
     uint8_t* seg_bytes = reinterpret_cast<uint8_t*>(seg);
     const uint32_t tid = threadIdx.x, lane = tid & 31;
+    // the segment arrives by one bulk copy completing on this barrier
+    __shared__ __align__(8) uint64_t seg_bar;
+    if (tid == 0) {
+        mbar_init(&seg_bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t seg_phase = 0;
     uint32_t n_ok = 0;
     for (uint64_t s = blockIdx.x; s < nseg; s += gridDim.x) {
         const uint32_t lo = start[s], hi = start[s + 1];
@@ -1175,23 +1186,26 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
         const uint64_t left = t.nb_mask + 1 - (s << sb_log2);
         const uint32_t nbk = left < sb ? static_cast<uint32_t>(left) : static_cast<uint32_t>(sb);
         const uint32_t words = nbk * WPB;
-        if (words % 2 == 0) {
-            const ulonglong2* g2 = reinterpret_cast<const ulonglong2*>(gseg);
-            ulonglong2* s2 = reinterpret_cast<ulonglong2*>(seg);
-            const uint32_t pairs = words / 2;
-            for (uint32_t w0 = tid; w0 < pairs; w0 += blockDim.x * 8) {
-                ulonglong2 v[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    if (w0 + j * blockDim.x < pairs) v[j] = __ldcs(g2 + w0 + j * blockDim.x);
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    if (w0 + j * blockDim.x < pairs) s2[w0 + j * blockDim.x] = v[j];
+        bool staged = true;
+        if (words % 2 == 0) {  // a whole number of 16-byte units: one bulk copy
+            if (tid == 0) {
+                fence_proxy_async_smem();  // earlier accesses of this shared memory come first
+                mbar_arrive_expect_tx(&seg_bar, words * 8u);
+                bulk_g2s(seg, gseg, words * 8u, &seg_bar);
             }
+            staged = mbar_wait(&seg_bar, seg_phase, kMbarPollLimit);
         } else {
             for (uint32_t w = tid; w < words; w += blockDim.x) seg[w] = gseg[w];
         }
-        __syncthreads();
+        if (__syncthreads_or(!staged)) {
+            // the copy did not land within its poll bound: report it (the
+            // host returns CF_ERR_DEVICE), give the copy in flight a second
+            // bounded wait, and leave the segment untouched
+            if (tid == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_WAIT_LIMIT);
+            mbar_wait(&seg_bar, seg_phase, kMbarPollLimit);
+            break;
+        }
+        if (words % 2 == 0) seg_phase ^= 1u;
         // claim words from the staged segment (ranked: counters at zero)
         auto build_claims = [&]() {
             for (uint32_t b = tid; b < sb; b += blockDim.x)
