@@ -277,14 +277,19 @@ int ensure_workspace(cf_filter* f, uint64_t n, bool payload, SegWork* w) {
     const uint64_t fixed = ws_need(f, 0, grid, payload) + 4096;
     const uint64_t kMaxChunk = 1ull << 31;  // 32-bit positions and payloads
     uint64_t limit = f->ws_limit;
+    bool fits_held = false;  // automatic limit, and the whole batch fits the workspace already held
     if (limit == 0) {  // automatic: the whole batch when device memory allows
         const uint64_t whole = ws_need(f, std::min(n, kMaxChunk), grid, payload);
-        limit = whole <= f->ws_bytes ? f->ws_bytes : auto_workspace_limit(f);
+        fits_held = whole <= f->ws_bytes;
+        limit = fits_held ? f->ws_bytes : auto_workspace_limit(f);
     }
     uint64_t cap = 0, need = 0;
     for (;;) {
         cap = n;
-        if (limit > fixed) {
+        if (fits_held) {
+            // one chunk (the fit below is conservative and would split off a
+            // sliver of the batch)
+        } else if (limit > fixed) {
             const uint64_t fit = (limit - fixed) / (payload ? 25 : 16);
             if (cap > fit) cap = fit;
         } else {

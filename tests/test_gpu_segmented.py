@@ -159,6 +159,24 @@ def test_workspace_default_is_automatic_and_holds_the_whole_batch(cfb, orc):
         f.close()
 
 
+def test_repeated_batch_reuses_the_workspace_in_one_chunk(cfb, orc):
+    """A batch that fits the workspace an earlier call left is not split: the
+    same fill, repeated on the cleared table, launches exactly the kernels the
+    first one did (a split would add a second radix / segment chain)."""
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, 1 << 22)
+    try:
+        keys = dev(orc.splitmix64(93, int(0.95 * f.capacity())))
+        counts = []
+        for _ in range(3):
+            f.clear()
+            before = cfb.launch_count()
+            assert f.insertManySorted(keys) == keys.numel()
+            counts.append(cfb.launch_count() - before)
+        assert counts[0] == counts[1] == counts[2], counts
+    finally:
+        f.close()
+
+
 LOOKUP = [(8, 16, 16), (8, 8, 16), (8, 32, 8), (4, 16, 16), (8, 16, 4), (8, 8, 64), (8, 16, 32), (8, 32, 2),
           (8, 8, 8), (4, 32, 16)]
 
