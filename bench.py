@@ -790,10 +790,25 @@ def run_b200(args, w: dict) -> dict | None:
             if k:  # first pass warms the pinned pages
                 times.append(time.perf_counter() - t0)
         t = max_over_ranks(world, statistics.mean(times))
+        # the PCIe ceiling: a plain copy of fill keys (2 GiB at most) from pinned
+        # host memory, CUDA events on the copy stream, best of three
+        nb = min(n_fill, 1 << 28)
+        h2d_rates = []
+        for _ in range(3):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(copy)
+            with torch.cuda.stream(copy):
+                d_fill[:nb].copy_(h_fill[:nb], non_blocking=True)
+            ev[1].record(copy)
+            ev[1].synchronize()
+            h2d_rates.append(8 * nb / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e9)
+        h2d_copy = max(h2d_rates)
+        h2d_achieved = 8 * keys_per_step / t / 1e9
         del h_fill, h_query, h_del, h_out
         release_pinned()
         e2e = {"value": all_keys / args.steps / t / 1e9, "unit": "Gkeys/s",
                "h2d_bytes_per_step": 8 * keys_per_step, "d2h_bytes_per_step": n_q + 3 * 8 * 16,
+               "h2d_achieved_gbs": h2d_achieved, "h2d_copy_gbs": h2d_copy, "frac_of_h2d_copy": h2d_achieved / h2d_copy,
                "ms_per_step": t * 1e3, "steps": n_e2e,
                "path": f"synchronous C-ABI calls ({'cf_insert_sorted' if sorted_fill else 'cf_insert'} in {nchunk} "
                        "chunks, cf_contains, cf_delete); inputs copied from pinned host memory on a copy stream that "
@@ -1750,9 +1765,11 @@ def run_gather(args) -> dict:
 
 def run_lookup_paths(args, w: dict) -> dict:
     """Lookups and deletes of the workload on each execution path, on the same
-    filled table: random probes, segment-staged and region-staged
-    (CF_OPT_STAGING), CUDA events per call, with the lookup results required
-    to be identical across paths and every delete to succeed."""
+    filled table: random probes (one lane per key, and every warp-cooperative
+    width CF_OPT_PROBE_WIDTH the geometry supports), segment-staged and
+    region-staged (CF_OPT_STAGING), CUDA events per call, with the lookup
+    results required to be identical across paths and every delete to
+    succeed."""
     import torch
 
     from __graft_entry__ import package
@@ -1773,9 +1790,15 @@ def run_lookup_paths(args, w: dict) -> dict:
     ref_out = None
     rows = []
     peak, _ = measured_peak()
-    for name, mode in (("random probes", cfb.STAGING_RANDOM), ("segment-staged", cfb.STAGING_SEGMENT),
-                       ("region-staged", cfb.STAGING_REGION)):
+    bb = w["bits"] * w["bs"] // 8
+    coop = [k for k in (2, 4, 8, 16, 32) if bb % k == 0 and bb // k in (4, 8) and w["bs"] <= 64]
+    paths = [("random probes", cfb.STAGING_RANDOM, 0)]
+    paths += [(f"random probes, {k} lanes per key (warp-cooperative, ballot / shuffle)", cfb.STAGING_RANDOM, k)
+              for k in coop]
+    paths += [("segment-staged", cfb.STAGING_SEGMENT, 0), ("region-staged", cfb.STAGING_REGION, 0)]
+    for name, mode, width in paths:
         f.setOption(cfb.OPT_STAGING, mode)
+        f.setOption(cfb.OPT_PROBE_WIDTH, width)
         con, dl = [], []
         for k in range(args.warmup + args.steps):
             e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -1787,8 +1810,10 @@ def run_lookup_paths(args, w: dict) -> dict:
             torch.cuda.synchronize()
             removed = int(d_out.sum().item())
             f.setOption(cfb.OPT_STAGING, cfb.STAGING_AUTO)
+            f.setOption(cfb.OPT_PROBE_WIDTH, 0)
             f.insertMany(dele, stream=stream)  # put the deleted keys back (untimed)
             f.setOption(cfb.OPT_STAGING, mode)
+            f.setOption(cfb.OPT_PROBE_WIDTH, width)
             if k >= args.warmup:
                 con.append(e[0].elapsed_time(e[1]))
                 dl.append(e[1].elapsed_time(e[2]))
@@ -1796,7 +1821,7 @@ def run_lookup_paths(args, w: dict) -> dict:
             ref_out = q_out.clone()
         q_primary = f.probe_count(query, stream=stream)
         con_bytes = query.numel() * 9 + 32 * (2 * query.numel() - q_primary)
-        rows.append({"path": name, "contains_ms": statistics.median(con),
+        rows.append({"path": name, "probe_width": max(width, 1), "contains_ms": statistics.median(con),
                      "contains_gkeys_s": query.numel() / statistics.median(con) / 1e6,
                      "contains_frac_sector_roofline": con_bytes / (statistics.median(con) / 1e3) / 1e9 / peak,
                      "delete_ms": statistics.median(dl), "delete_gkeys_s": dele.numel() / statistics.median(dl) / 1e6,

@@ -54,6 +54,7 @@ OPT_LOOKUP_KPT = 9
 OPT_PERSISTENT = 10
 OPT_CHAIN_HISTOGRAM = 11
 OPT_ROUND1_CAP = 12
+OPT_PROBE_WIDTH = 13
 NEVER = (1 << 64) - 1
 
 # cf_staging values (OPT_STAGING)

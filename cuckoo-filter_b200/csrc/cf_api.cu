@@ -49,6 +49,7 @@ struct cf_filter {
     uint32_t staging;       // CF_OPT_STAGING (cf_staging)
     uint64_t rg_bytes;      // CF_OPT_REGION_BYTES (0 = kRgRegionBytes)
     uint32_t lookup_kpt;    // CF_OPT_LOOKUP_KPT (0 = default)
+    uint32_t probe_width;   // CF_OPT_PROBE_WIDTH (0 or 1 = one lane per key)
     uint32_t persistent;    // CF_OPT_PERSISTENT (0 = one tile per CTA, 1 = persistent grid)
     uint32_t chain_hist;    // CF_OPT_CHAIN_HISTOGRAM
 };
@@ -634,6 +635,7 @@ int cf_contains_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_o
     }
     LaunchCfg L = launch(f, KID_CONTAINS, stream);
     L.kpt = static_cast<int>(f->lookup_kpt);
+    L.width = static_cast<int>(f->probe_width);
     CF_CUDA(f->ops->contains(dev(f), d_keys, n, d_out, L), "contains launch");
     return CF_OK;
 }
@@ -653,7 +655,9 @@ int cf_delete_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out
         case PATH_SEGMENT: return run_segmented(f, SEG_DELETE, d_keys, n, d_out, stream);
         default: break;
     }
-    CF_CUDA(f->ops->remove(dev(f), d_keys, n, d_out, launch(f, KID_DELETE, stream)), "delete launch");
+    LaunchCfg L = launch(f, KID_DELETE, stream);
+    L.width = static_cast<int>(f->probe_width);
+    CF_CUDA(f->ops->remove(dev(f), d_keys, n, d_out, L), "delete launch");
     return CF_OK;
 }
 
@@ -781,6 +785,14 @@ int cf_set_option(cf_filter* f, int option, uint64_t value) {
                 return fail(CF_ERR_INVALID, "lookup keys per thread must be 0, 1, 2 or 4");
             f->lookup_kpt = static_cast<uint32_t>(value);
             return CF_OK;
+        case CF_OPT_PROBE_WIDTH:
+            if (value > 1 && ((value & (value - 1)) != 0 || value > 32 ||
+                              !((f->ops->coop_widths >> __builtin_ctzll(value)) & 1u)))
+                return fail(CF_ERR_INVALID,
+                            "probe width %llu not supported for %u-byte buckets (lanes of 4 or 8 bytes, at most 64 slots)",
+                            static_cast<unsigned long long>(value), f->ops->bucket_bytes);
+            f->probe_width = static_cast<uint32_t>(value);
+            return CF_OK;
         case CF_OPT_PERSISTENT:
             if (value > 1) return fail(CF_ERR_INVALID, "persistent must be 0 or 1");
             f->persistent = static_cast<uint32_t>(value);
@@ -817,6 +829,7 @@ int cf_get_option(cf_filter* f, int option, uint64_t* value) {
         case CF_OPT_REGION_BYTES: *value = f->rg_bytes ? f->rg_bytes : kRgRegionBytes; return CF_OK;
         case CF_OPT_REGION_COUNT: *value = f->rgeom.nreg; return CF_OK;
         case CF_OPT_LOOKUP_KPT: *value = f->lookup_kpt; return CF_OK;
+        case CF_OPT_PROBE_WIDTH: *value = f->probe_width; return CF_OK;
         case CF_OPT_PERSISTENT: *value = f->persistent; return CF_OK;
         case CF_OPT_ROUND1_CAP: *value = f->round1_cap; return CF_OK;
         case CF_OPT_CHAIN_HISTOGRAM: *value = f->chain_hist; return CF_OK;

@@ -551,6 +551,219 @@ __global__ void __launch_bounds__(512) k_delete(DevTable t, const typename C::Ke
     if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
 }
 
+// ------------------------------------------------- warp-cooperative probing
+//
+// containsMany / deleteMany with W lanes per key (CF_OPT_PROBE_WIDTH): a group
+// of W consecutive lanes owns KPT consecutive keys, and lane r of the group
+// loads bytes [r*PB, (r+1)*PB) of each bucket (PB = bucket_bytes / W, 4 or 8).
+// The group votes by ballot (lookups) or assembles the bucket's slot mask by
+// shuffles (deletes), so a key's bucket is one coalesced 32-lane request
+// shared by W lanes instead of one lane's 16- or 32-byte vector load.
+
+template <class C, int W>
+struct CoopGeom {
+    static constexpr int PB = C::bucket_bytes / W;          // bytes of a bucket per lane
+    static constexpr int spl = PB * 8 / C::bits;            // slots per lane
+    static constexpr bool ok = W >= 2 && W <= 32 && C::bucket_bytes % W == 0 && (PB == 4 || PB == 8) && C::bs <= 64;
+};
+
+// Lookup piece test: does the `PB`-byte piece (zero-extended into 64 bits)
+// hold tag fp?  Zero-extended lanes XOR the replicated tag are non-zero, so
+// they never match.
+template <class C, int PB>
+__device__ __forceinline__ bool piece_has(uint64_t piece, uint32_t fp) {
+    const uint64_t rep = replicate<C::bits>(fp);
+    uint64_t z = zero_lanes<C::bits>(piece ^ rep);
+    if constexpr (PB < 8) z &= (1ull << (8 * PB)) - 1ull;
+    return z != 0;
+}
+
+// Slots of a piece holding fp, as bits 0 .. PB*8/bits - 1.
+template <class C, int PB>
+__device__ __forceinline__ uint32_t piece_slots(uint64_t piece, uint32_t fp) {
+    constexpr int spl = PB * 8 / C::bits;
+    const uint64_t z = zero_lanes<C::bits>(piece ^ replicate<C::bits>(fp));
+    uint32_t m = 0;
+#pragma unroll
+    for (int l = 0; l < spl; ++l) m |= static_cast<uint32_t>((z >> (l * C::bits + C::bits - 1)) & 1u) << l;
+    return m;
+}
+
+template <int PB>
+__device__ __forceinline__ uint64_t load_piece(const uint8_t* p) {
+    if constexpr (PB == 8) {
+        uint64_t v;
+        asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
+        return v;
+    } else {
+        uint32_t v;
+        asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+        return v;
+    }
+}
+
+// As load_piece, coherent with the compare-and-swaps of the same launch.
+template <int PB>
+__device__ __forceinline__ uint64_t load_piece_rlx(const uint8_t* p) {
+    if constexpr (PB == 8) {
+        uint64_t v;
+        asm volatile("ld.relaxed.gpu.global.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+        return v;
+    } else {
+        uint32_t v;
+        asm volatile("ld.relaxed.gpu.global.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        return v;
+    }
+}
+
+// containsMany (CuckooFilter.cuh:1088-1098, :1143-1155) with W lanes per key.
+template <class C, int KPT, int W>
+__global__ void __launch_bounds__(512) k_contains_coop(DevTable t, const typename C::Key* __restrict__ keys,
+                                                       uint64_t n, uint8_t* __restrict__ out, bool out_vec) {
+    using G = CoopGeom<C, W>;
+    static_assert(G::ok, "W lanes of 4 or 8 bytes each cover the bucket");
+    const uint32_t lane = threadIdx.x & 31, r = lane % W;
+    const uint32_t gmask = (W == 32 ? 0xFFFFFFFFu : ((1u << W) - 1u)) << (lane - r);
+    const uint64_t tile = static_cast<uint64_t>(blockDim.x / W) * KPT;
+    // the trip count is uniform over the block: every lane reaches every ballot
+    for (uint64_t base = blockIdx.x * tile; base < n; base += static_cast<uint64_t>(gridDim.x) * tile) {
+        const uint64_t k0 = base + static_cast<uint64_t>(threadIdx.x / W) * KPT;
+        uint64_t b[KPT], piece[KPT];
+        uint32_t fp[KPT];
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            b[j] = 0;
+            fp[j] = 0;
+            piece[j] = 0;
+            if (k0 + j < n) {
+                candidates<C>(static_cast<uint64_t>(keys[k0 + j]), t.nb_mask, b[j], fp[j]);
+                piece[j] = load_piece<G::PB>(t.buckets + b[j] * C::bucket_bytes + r * G::PB);
+            }
+        }
+        uint32_t hit = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            const bool mine = k0 + j < n && piece_has<C, G::PB>(piece[j], fp[j]);
+            if (__ballot_sync(0xFFFFFFFFu, mine) & gmask) hit |= 1u << j;
+        }
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            if (k0 + j < n && !((hit >> j) & 1u)) {
+                b[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
+                fp[j] = alt_tag<C>(fp[j]);
+                piece[j] = load_piece<G::PB>(t.buckets + b[j] * C::bucket_bytes + r * G::PB);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            const bool mine = k0 + j < n && !((hit >> j) & 1u) && piece_has<C, G::PB>(piece[j], fp[j]);
+            if (__ballot_sync(0xFFFFFFFFu, mine) & gmask) hit |= 1u << j;
+        }
+        if (r == 0 && k0 < n) store_results<KPT>(out, k0, n, out_vec, hit);
+    }
+}
+
+// tryRemoveAtBucket (first slot holding fp in the reference's scan order) for
+// the keys of `pend`, W lanes per key: the group assembles the bucket's slot
+// mask from its pieces, and the lane holding the chosen slot clears it with a
+// compare-and-swap on its own 4- or 8-byte word.  A lost race refreshes that
+// lane's piece and the group chooses again.  Keys removed are set in `done`.
+template <class C, int W, int KPT>
+__device__ __forceinline__ void coop_remove(const DevTable& t, const uint64_t (&b)[KPT], const uint32_t (&fp)[KPT],
+                                            uint64_t (&piece)[KPT], uint32_t pend, uint32_t& done, bool& err,
+                                            uint32_t r, uint32_t gmask) {
+    using G = CoopGeom<C, W>;
+    using M = SlotMask<C>;
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        bool want = (pend >> j) & 1u;  // uniform over the group
+        for (int it = 0; it < kCasRetryLimit; ++it) {
+            if (!__any_sync(0xFFFFFFFFu, want)) break;
+            M m = want ? static_cast<M>(static_cast<M>(piece_slots<C, G::PB>(piece[j], fp[j])) << (r * G::spl))
+                       : static_cast<M>(0);
+#pragma unroll
+            for (int d = 1; d < W; d <<= 1) m |= __shfl_xor_sync(0xFFFFFFFFu, m, d);
+            bool ok = false;
+            if (want && m) {
+                const uint32_t slot = scan_slot<C>(m, fp[j]);
+                if (slot / G::spl == r) {
+                    uint8_t* p = t.buckets + b[j] * C::bucket_bytes + r * G::PB;
+                    const uint64_t cur = piece[j];
+                    const uint64_t des = cur & ~(lane_mask << ((slot % G::spl) * C::bits));
+                    uint64_t old;
+                    if constexpr (G::PB == 8)
+                        old = atomicCAS(reinterpret_cast<unsigned long long*>(p), cur, des);
+                    else
+                        old = atomicCAS(reinterpret_cast<unsigned int*>(p), static_cast<unsigned int>(cur),
+                                        static_cast<unsigned int>(des));
+                    ok = old == cur;
+                    if (!ok) piece[j] = old;
+                }
+            }
+            const uint32_t vote = __ballot_sync(0xFFFFFFFFu, ok) & gmask;
+            if (want && !m) {
+                want = false;  // no copy of fp in this bucket
+            } else if (want && vote) {
+                want = false;
+                done |= 1u << j;
+            }
+        }
+        if (want) err = true;
+    }
+}
+
+// deleteMany (CuckooFilter.cuh:805-848, :1157-1183) with W lanes per key.
+template <class C, int KPT, int W>
+__global__ void __launch_bounds__(512) k_delete_coop(DevTable t, const typename C::Key* __restrict__ keys, uint64_t n,
+                                                     uint8_t* __restrict__ out, bool out_vec) {
+    using G = CoopGeom<C, W>;
+    static_assert(G::ok, "W lanes of 4 or 8 bytes each cover the bucket");
+    const uint32_t lane = threadIdx.x & 31, r = lane % W;
+    const uint32_t gmask = (W == 32 ? 0xFFFFFFFFu : ((1u << W) - 1u)) << (lane - r);
+    const uint64_t tile = static_cast<uint64_t>(blockDim.x / W) * KPT;
+    uint32_t removed = 0;
+    bool err = false;
+    for (uint64_t base = blockIdx.x * tile; base < n; base += static_cast<uint64_t>(gridDim.x) * tile) {
+        const uint64_t k0 = base + static_cast<uint64_t>(threadIdx.x / W) * KPT;
+        uint64_t b[KPT], piece[KPT];
+        uint32_t fp[KPT];
+        uint32_t pend = 0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            b[j] = 0;
+            fp[j] = 0;
+            piece[j] = 0;
+            if (k0 + j < n) {
+                candidates<C>(static_cast<uint64_t>(keys[k0 + j]), t.nb_mask, b[j], fp[j]);
+                piece[j] = load_piece_rlx<G::PB>(t.buckets + b[j] * C::bucket_bytes + r * G::PB);
+                pend |= 1u << j;
+            }
+        }
+        uint32_t done = 0;
+        coop_remove<C, W, KPT>(t, b, fp, piece, pend, done, err, r, gmask);
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            if (((pend >> j) & 1u) && !((done >> j) & 1u)) {
+                b[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
+                fp[j] = alt_tag<C>(fp[j]);
+                piece[j] = load_piece_rlx<G::PB>(t.buckets + b[j] * C::bucket_bytes + r * G::PB);
+            }
+        }
+        coop_remove<C, W, KPT>(t, b, fp, piece, pend & ~done, done, err, r, gmask);
+        if (r == 0) {
+            removed += __popc(done);
+            if (out && k0 < n) store_results<KPT>(out, k0, n, out_vec, done);
+        }
+    }
+    const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, removed);
+    if ((threadIdx.x & 31) == 0 && s) {
+        atomicAdd(&t.ctr[CTR_REMOVED], static_cast<unsigned long long>(s));
+        atomicAdd(&t.ctr[CTR_OCCUPIED], ~static_cast<unsigned long long>(s) + 1ull);  // -= s
+    }
+    if (__any_sync(0xFFFFFFFFu, err) && (threadIdx.x & 31) == 0) atomicOr(&t.ctr[CTR_ERROR], ERR_CAS_LIMIT);
+}
+
 // Eviction for one key whose two buckets were full (CuckooFilter::insert,
 // CuckooFilter.cuh:1066-1071): start at i1 if the tag is even, else at i2.
 template <class C>

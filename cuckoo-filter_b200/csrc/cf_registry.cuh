@@ -85,6 +85,7 @@ struct LaunchCfg {
     int block;
     int max_grid;        // persistent grid for this kernel and block size
     int kpt = 0;         // keys per thread of the lookup kernel (1, 2, 4; 0 = kContainsKPT)
+    int width = 1;       // lanes per key of lookups and deletes (CF_OPT_PROBE_WIDTH; 1 = one lane per key)
     bool full_grid = true;   // one tile per CTA instead of a persistent grid
 };
 
@@ -92,6 +93,7 @@ struct OpsTable {
     uint32_t key_bytes, bits, bucket_size, word_bytes, alt_policy;
     uint32_t bucket_bytes;
     int kpt[KID_COUNT_KERNELS];
+    uint32_t coop_widths;  // CF_OPT_PROBE_WIDTH values above 1 this geometry supports (bit log2(W))
     cudaError_t (*contains)(const DevTable&, const void*, uint64_t, uint8_t*, const LaunchCfg&);
     cudaError_t (*remove)(const DevTable&, const void*, uint64_t, uint8_t*, const LaunchCfg&);
     cudaError_t (*insert)(const DevTable&, const void*, uint64_t, uint8_t*, const LaunchCfg&, uint32_t policy_bfs,
@@ -181,8 +183,48 @@ struct Launchers {
                                                          aligned(keys, key_vec_align<C, K>()), aligned(out, K)); CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
+    // warp-cooperative lookups and deletes: W lanes per key, kCoopKPT keys per group
+    static constexpr int kCoopKPT = 4;
+    template <int W>
+    static cudaError_t contains_w(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
+        if constexpr (CoopGeom<C, W>::ok) {
+            const int groups = L.block / W;
+            const int grid = L.full_grid ? full_grid_for(n, groups, kCoopKPT) : grid_for(n, groups, kCoopKPT, L.max_grid);
+            { k_contains_coop<C, kCoopKPT, W><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
+                                                                             aligned(out, kCoopKPT)); CF_COUNT_LAUNCH(); }
+            return cudaGetLastError();
+        } else {
+            return cudaErrorInvalidValue;
+        }
+    }
+    template <int W>
+    static cudaError_t remove_w(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
+        if constexpr (CoopGeom<C, W>::ok) {
+            const int groups = L.block / W;
+            const int grid = L.full_grid ? full_grid_for(n, groups, kCoopKPT) : grid_for(n, groups, kCoopKPT, L.max_grid);
+            { k_delete_coop<C, kCoopKPT, W><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
+                                                                           aligned(out, kCoopKPT)); CF_COUNT_LAUNCH(); }
+            return cudaGetLastError();
+        } else {
+            return cudaErrorInvalidValue;
+        }
+    }
+    // the probe widths this geometry supports: bit log2(W) set for W lanes per key
+    static constexpr uint32_t coop_widths() {
+        return (CoopGeom<C, 2>::ok ? 1u << 1 : 0u) | (CoopGeom<C, 4>::ok ? 1u << 2 : 0u) |
+               (CoopGeom<C, 8>::ok ? 1u << 3 : 0u) | (CoopGeom<C, 16>::ok ? 1u << 4 : 0u) |
+               (CoopGeom<C, 32>::ok ? 1u << 5 : 0u);
+    }
     static cudaError_t contains(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
         if (n == 0) return cudaSuccess;
+        switch (L.width) {
+            case 2: return contains_w<2>(t, keys, n, out, L);
+            case 4: return contains_w<4>(t, keys, n, out, L);
+            case 8: return contains_w<8>(t, keys, n, out, L);
+            case 16: return contains_w<16>(t, keys, n, out, L);
+            case 32: return contains_w<32>(t, keys, n, out, L);
+            default: break;
+        }
         switch (L.kpt) {
             case 1: return contains_k<1>(t, keys, n, out, L);
             case 2: return contains_k<2>(t, keys, n, out, L);
@@ -191,6 +233,14 @@ struct Launchers {
     }
     static cudaError_t remove(const DevTable& t, const void* keys, uint64_t n, uint8_t* out, const LaunchCfg& L) {
         if (n == 0) return cudaSuccess;
+        switch (L.width) {
+            case 2: return remove_w<2>(t, keys, n, out, L);
+            case 4: return remove_w<4>(t, keys, n, out, L);
+            case 8: return remove_w<8>(t, keys, n, out, L);
+            case 16: return remove_w<16>(t, keys, n, out, L);
+            case 32: return remove_w<32>(t, keys, n, out, L);
+            default: break;
+        }
         constexpr int K = DKPT;
         const int grid = L.full_grid ? full_grid_for(n, L.block, K) : grid_for(n, L.block, K, L.max_grid);
         { k_delete<C, K><<<grid, L.block, 0, L.stream>>>(t, static_cast<const Key*>(keys), n, out,
@@ -593,6 +643,7 @@ struct Launchers {
         o.kpt[KID_CONTAINS] = CKPT;
         o.kpt[KID_DELETE] = DKPT;
         o.kpt[KID_INSERT] = IKPT;
+        o.coop_widths = coop_widths();
         o.contains = contains;
         o.remove = remove;
         o.insert = insert;

@@ -189,63 +189,74 @@ __global__ void __launch_bounds__(kRsHistThreads, 3)
     }
 }
 
-// Exclusive scan of `count` uint32 values in place (one CTA of 1024 threads,
-// sixteen consecutive values per thread per step, read and written as
-// 16-byte vectors when the array is 16-byte aligned).
+// Exclusive scan of `count` uint32 values in place (sums wrap modulo 2^32),
+// one CTA of 1024 threads.  Each warp owns one contiguous span of whole rows
+// (a row: 32 lanes x 4 values, one coalesced 16-byte load per lane when the
+// array is 16-byte aligned), with eight rows in flight per lane: the warp
+// sums its span, the 32 warp sums are scanned, and the warp reads its span
+// again and writes it scanned row by row.  Two passes of a few dependent
+// round trips each, instead of one block-synchronized step per 16K values.
 static __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* v, uint32_t count) {
-    constexpr uint32_t V = 16;
+    constexpr uint32_t R = 8;    // rows in flight per lane
+    constexpr uint32_t ROW = 128;
     __shared__ uint32_t warp_tot[32];
-    __shared__ uint32_t carry;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool vec = (reinterpret_cast<uintptr_t>(v) & 15) == 0;
-    if (threadIdx.x == 0) carry = 0;
+    const uint64_t n = count;
+    const uint64_t span = ((n + 31) / 32 + ROW - 1) / ROW * ROW;
+    const uint64_t b = warp * span < n ? warp * span : n;
+    const uint64_t e = b + span < n ? b + span : n;
+    // the four values from index i (16-byte aligned when vec; zero past e)
+    auto ld4 = [&](uint64_t i) -> uint4 {
+        if (vec && i + 4 <= e) return *reinterpret_cast<const uint4*>(v + i);
+        uint4 x;
+        x.x = i < e ? v[i] : 0u;
+        x.y = i + 1 < e ? v[i + 1] : 0u;
+        x.z = i + 2 < e ? v[i + 2] : 0u;
+        x.w = i + 3 < e ? v[i + 3] : 0u;
+        return x;
+    };
+    uint32_t s = 0;
+    for (uint64_t row = b; row < e; row += ROW * R) {
+        uint4 x[R];
+#pragma unroll
+        for (uint32_t q = 0; q < R; ++q) x[q] = ld4(row + q * ROW + lane * 4);
+#pragma unroll
+        for (uint32_t q = 0; q < R; ++q) s += x[q].x + x[q].y + x[q].z + x[q].w;
+    }
+    s = __reduce_add_sync(0xFFFFFFFFu, s);
+    if (lane == 0) warp_tot[warp] = s;
     __syncthreads();
-    for (uint32_t base = 0; base < count; base += 1024 * V) {
-        const uint32_t i0 = base + threadIdx.x * V;
-        const bool whole = vec && i0 + V <= count;
-        uint32_t x[V], s = 0;
-        if (whole) {
+    if (warp == 0) {
+        const uint32_t t = warp_tot[lane];
+        warp_tot[lane] = warp_inclusive_scan(t) - t;
+    }
+    __syncthreads();
+    uint32_t carry = warp_tot[warp];
+    for (uint64_t row = b; row < e; row += ROW * R) {
+        uint4 x[R];
 #pragma unroll
-            for (uint32_t q = 0; q < V / 4; ++q) {
-                const uint4 u = reinterpret_cast<const uint4*>(v + i0)[q];
-                x[4 * q] = u.x;
-                x[4 * q + 1] = u.y;
-                x[4 * q + 2] = u.z;
-                x[4 * q + 3] = u.w;
+        for (uint32_t q = 0; q < R; ++q) x[q] = ld4(row + q * ROW + lane * 4);
+#pragma unroll
+        for (uint32_t q = 0; q < R; ++q) {
+            const uint32_t ls = x[q].x + x[q].y + x[q].z + x[q].w;
+            const uint32_t incl = warp_inclusive_scan(ls);
+            uint4 o;
+            o.x = carry + incl - ls;
+            o.y = o.x + x[q].x;
+            o.z = o.y + x[q].y;
+            o.w = o.z + x[q].z;
+            const uint64_t i = row + q * ROW + lane * 4;
+            if (vec && i + 4 <= e) {
+                *reinterpret_cast<uint4*>(v + i) = o;
+            } else {
+                if (i < e) v[i] = o.x;
+                if (i + 1 < e) v[i + 1] = o.y;
+                if (i + 2 < e) v[i + 2] = o.z;
+                if (i + 3 < e) v[i + 3] = o.w;
             }
-        } else {
-#pragma unroll
-            for (uint32_t j = 0; j < V; ++j) x[j] = i0 + j < count ? v[i0 + j] : 0u;
+            carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
         }
-#pragma unroll
-        for (uint32_t j = 0; j < V; ++j) s += x[j];
-        const uint32_t incl = warp_inclusive_scan(s);
-        if (lane == 31) warp_tot[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t t = warp_tot[lane];
-            warp_tot[lane] = warp_inclusive_scan(t) - t;
-        }
-        __syncthreads();
-        uint32_t run = carry + warp_tot[warp] + incl - s;
-#pragma unroll
-        for (uint32_t j = 0; j < V; ++j) {
-            const uint32_t c = x[j];
-            x[j] = run;
-            run += c;
-        }
-        if (whole) {
-#pragma unroll
-            for (uint32_t q = 0; q < V / 4; ++q)
-                reinterpret_cast<uint4*>(v + i0)[q] = make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
-        } else {
-#pragma unroll
-            for (uint32_t j = 0; j < V; ++j)
-                if (i0 + j < count) v[i0 + j] = x[j];
-        }
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = run;
-        __syncthreads();
     }
 }
 

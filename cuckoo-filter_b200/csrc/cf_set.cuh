@@ -70,30 +70,6 @@ __device__ __forceinline__ void set_add_ctr(const DevTable* __restrict__ descs, 
     }
 }
 
-// Lookup piece test: does the `PB`-byte piece (zero-extended into 64 bits)
-// hold tag fp?  Zero-extended lanes XOR the replicated tag are non-zero, so
-// they never match.
-template <class C, int PB>
-__device__ __forceinline__ bool piece_has(uint64_t piece, uint32_t fp) {
-    const uint64_t rep = replicate<C::bits>(fp);
-    uint64_t z = zero_lanes<C::bits>(piece ^ rep);
-    if constexpr (PB < 8) z &= (1ull << (8 * PB)) - 1ull;
-    return z != 0;
-}
-
-template <int PB>
-__device__ __forceinline__ uint64_t load_piece(const uint8_t* p) {
-    if constexpr (PB == 8) {
-        uint64_t v;
-        asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
-        return v;
-    } else {
-        uint32_t v;
-        asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
-        return v;
-    }
-}
-
 // containsMany over the set, W = 1: each thread owns KPT consecutive keys.
 template <class C, int KPT>
 __global__ void __launch_bounds__(512) k_set_contains1(const DevTable* __restrict__ descs,

@@ -240,7 +240,18 @@ typedef enum cf_option {
      * primary bucket before eviction; bucket_size = no limit and no third
      * round (the reference's primary-first order: a key goes to its
      * alternate bucket only when its primary is full).  1..bucket_size. */
-    CF_OPT_ROUND1_CAP = 12
+    CF_OPT_ROUND1_CAP = 12,
+    /* Lanes per key of the random-probe lookups and deletes
+     * (containsMany / deleteMany, CuckooFilter.cuh:1143-1183).  0 or 1
+     * (default): one lane per key, which loads the whole bucket as one 16- or
+     * 32-byte vector.  W in {2, 4, 8, 16, 32} with bucket_bytes / W equal to 4
+     * or 8 and at most 64 slots per bucket (otherwise CF_ERR_INVALID): W
+     * consecutive lanes share a key, each loading its 4- or 8-byte piece of
+     * the bucket; a lookup votes by ballot, and a delete assembles the
+     * bucket's slot mask by shuffles and clears the reference's slot with one
+     * compare-and-swap on the piece that holds it.  Results are the same for
+     * every width. */
+    CF_OPT_PROBE_WIDTH = 13
 } cf_option;
 
 /* Eviction-chain-length histogram since creation, cf_clear or cf_reset_stats,
