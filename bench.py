@@ -301,7 +301,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -309,7 +309,7 @@ class ClockSampler:
     def __exit__(self, *exc):
         self.lines = []
         if self.proc:
-            time.sleep(0.25)
+            time.sleep(0.05)  # the sample in progress, not the idle time after the region
             self.proc.terminate()
             try:
                 out, _ = self.proc.communicate(timeout=5)
@@ -1982,7 +1982,7 @@ def run_reference_gpu(args, w: dict) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large")

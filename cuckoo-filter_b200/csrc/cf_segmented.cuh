@@ -104,18 +104,20 @@ __device__ __forceinline__ uint64_t chunk_of(uint64_t n, uint32_t parts) {
 // SEGS (last pass of a sort whose earlier passes ordered the items by the
 // lower `lo_bits` bits of the segment id): also counts every segment,
 // seg_count[(digit << lo_bits) | lower] += 1, so the segment starts are one
-// scan away.  Within a CTA's chunk the lower bits never decrease, so a step of
-// items that all share them is counted in shared memory and flushed when they
-// change; a step that straddles a change counts straight into global memory.
+// scan away.  Within a CTA's chunk the lower bits never decrease: while they
+// stay the same, the run's per-digit counts are the growth of the digit
+// counts since the last flush (snap), added to seg_count when the run ends;
+// a step that straddles a change adds its items to seg_count one by one.
+// One shared-memory atomic per item either way.
 template <class C, bool KEYS, bool SEGS>
 __global__ void __launch_bounds__(kRsHistThreads, 3)
     k_rs_hist(const void* src, uint64_t nb_mask, uint64_t n, const unsigned long long* n_dev, int shift,
               uint32_t* hist, uint64_t* ent_out, int lo_bits, uint32_t* seg_count) {
     __shared__ uint32_t cnt[kRadix];
-    __shared__ uint32_t run_cnt[SEGS ? kRadix : 1];
+    __shared__ uint32_t snap[SEGS ? kRadix : 1];
     for (int i = threadIdx.x; i < kRadix; i += blockDim.x) {
         cnt[i] = 0;
-        if constexpr (SEGS) run_cnt[i] = 0;
+        if constexpr (SEGS) snap[i] = 0;
     }
     __syncthreads();
     const uint64_t m = item_count(n, n_dev);
@@ -142,16 +144,18 @@ __global__ void __launch_bounds__(kRsHistThreads, 3)
                 lf = static_cast<uint32_t>(ent[b] >> lo_shift) & lo_mask;
                 ll = static_cast<uint32_t>(ent[last] >> lo_shift) & lo_mask;
             }
-            if (lf != cur) {
+            if (lf != cur || lf != ll) {  // the run ends here: flush it
                 __syncthreads();
                 for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
-                    if (run_cnt[d]) atomicAdd(&seg_count[(static_cast<uint32_t>(d) << lo_bits) | cur], run_cnt[d]);
-                    run_cnt[d] = 0;
+                    const uint32_t c = cnt[d] - snap[d];
+                    if (c) atomicAdd(&seg_count[(static_cast<uint32_t>(d) << lo_bits) | cur], c);
+                    snap[d] = cnt[d];
                 }
                 __syncthreads();
                 cur = lf;
             }
             straddle = lf != ll;
+            if (straddle) cur = ll;  // the run after this step
         }
         // every load of the step is issued before any key is hashed
         uint64_t e[U];
@@ -172,20 +176,26 @@ __global__ void __launch_bounds__(kRsHistThreads, 3)
                 const uint32_t d = static_cast<uint32_t>(e[j] >> shift) & (kRadix - 1);
                 atomicAdd(&cnt[d], 1u);
                 if constexpr (KEYS) ent_out[i] = e[j];
-                if constexpr (SEGS) {
-                    if (!straddle)
-                        atomicAdd(&run_cnt[d], 1u);
-                    else
+                if constexpr (SEGS)
+                    if (straddle)
                         atomicAdd(&seg_count[(d << lo_bits) | (static_cast<uint32_t>(e[j] >> lo_shift) & lo_mask)], 1u);
-                }
+            }
+        }
+        if constexpr (SEGS) {
+            if (straddle) {  // the step's items are in seg_count already: keep them out of the run
+                __syncthreads();
+                for (int d = threadIdx.x; d < kRadix; d += blockDim.x) snap[d] = cnt[d];
+                __syncthreads();
             }
         }
     }
     __syncthreads();
     for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
         hist[(static_cast<uint64_t>(d) * sgrid + cta) * kRsHistSub + part] = cnt[d];
-        if constexpr (SEGS)
-            if (run_cnt[d]) atomicAdd(&seg_count[(static_cast<uint32_t>(d) << lo_bits) | cur], run_cnt[d]);
+        if constexpr (SEGS) {
+            const uint32_t c = cnt[d] - snap[d];
+            if (c) atomicAdd(&seg_count[(static_cast<uint32_t>(d) << lo_bits) | cur], c);
+        }
     }
 }
 
