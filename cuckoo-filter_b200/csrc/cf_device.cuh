@@ -332,8 +332,9 @@ __device__ __forceinline__ void red_or_policy(uint32_t* p, uint32_t v, uint64_t 
 // ------------------------------------------- bulk copies (TMA) and mbarriers
 //
 // One-dimensional cp.async.bulk global -> shared copies completing on an
-// mbarrier's transaction count.  Source and destination must be 16-byte
-// aligned and the size a multiple of 16 bytes.  No multicast form is used.
+// mbarrier's transaction count, and shared -> global copies completing as
+// bulk async-groups.  Source and destination must be 16-byte aligned and the
+// size a multiple of 16 bytes.  No multicast form is used.
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -355,6 +356,18 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  "l"(src), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
+// One-dimensional cp.async.bulk shared -> global copy (bulk async-group
+// completion).  Both addresses 16-byte aligned, size a multiple of 16 bytes.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until this thread's committed bulk stores have read their shared-memory source.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Waits until this thread's committed bulk stores have completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // Waits until the phase with parity `parity` of `bar` completes.  Returns
 // false after `limit` unsuccessful polls (each poll may suspend the thread for
 // a hardware-defined interval), so a copy that never lands cannot hang the CTA.

@@ -1208,6 +1208,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
         const uint32_t nbk = left < sb ? static_cast<uint32_t>(left) : static_cast<uint32_t>(sb);
         const uint32_t words = nbk * WPB;
         bool staged = true;
+        if (tid == 0) bulk_wait_read();  // the previous segment's write-back has read the buffer
         if (words % 2 == 0) {  // a whole number of 16-byte units: one bulk copy
             if (tid == 0) {
                 fence_proxy_async_smem();  // earlier accesses of this shared memory come first
@@ -1216,6 +1217,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
             }
             staged = mbar_wait(&seg_bar, seg_phase, kMbarPollLimit);
         } else {
+            __syncthreads();
             for (uint32_t w = tid; w < words; w += blockDim.x) seg[w] = gseg[w];
         }
         if (__syncthreads_or(!staged)) {
@@ -1375,14 +1377,20 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
             }
         }
         if (words % 2 == 0) {
-            ulonglong2* g2 = reinterpret_cast<ulonglong2*>(gseg);
-            const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(seg);
-            for (uint32_t w = tid; w < words / 2; w += blockDim.x) __stcs(g2 + w, s2[w]);
+            // the segment leaves by one bulk copy, which reads the buffer
+            // while the CTA moves on (the next load waits for that read)
+            fence_proxy_async_smem();  // this thread's tag stores, before the copy reads them
+            __syncthreads();
+            if (tid == 0) {
+                bulk_s2g(gseg, seg, words * 8u);
+                bulk_commit();
+            }
         } else {
             for (uint32_t w = tid; w < words; w += blockDim.x) gseg[w] = seg[w];
         }
         __syncthreads();
     }
+    if (tid == 0) bulk_wait_all();
     flush_counter(&t.ctr[round == 2 ? CTR_SECONDARY : CTR_PRIMARY], n_ok);
     flush_counter(&t.ctr[CTR_OCCUPIED], n_ok);
 }
