@@ -157,3 +157,14 @@ def test_python_config_mirror(cfb):
     assert cfb.CuckooConfig(T="uint64", bitsPerTag=16, AltBucketPolicy="OffsetAltBucketPolicy").to_c().alt_policy == 2
     with pytest.raises(cfb.CuckooError):
         cfb.CuckooConfig(T="uint64", bitsPerTag=16, AltBucketPolicy="ModuloAltBucketPolicy").to_c()
+
+
+def test_python_option_constants_match_the_header(cfb):
+    """Every CF_OPT_* and CF_STAGING_* value of include/cuckoo_b200.h has a
+    Python constant of the same name (without the CF_ prefix) and value."""
+    text = open(os.path.join(ROOT, "include", "cuckoo_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    found = dict((m.group(1), int(m.group(2))) for m in re.finditer(r"\bCF_((?:OPT|STAGING)_\w+)\s*=\s*(\d+)", text))
+    assert "OPT_PROBE_WIDTH" in found and "STAGING_REGION" in found
+    for name, value in found.items():
+        assert getattr(cfb, name) == value, name
