@@ -50,6 +50,9 @@ struct cf_filter {
     uint64_t rg_bytes;      // CF_OPT_REGION_BYTES (0 = kRgRegionBytes)
     uint32_t lookup_kpt;    // CF_OPT_LOOKUP_KPT (0 = default)
     uint32_t probe_width;   // CF_OPT_PROBE_WIDTH (0 or 1 = one lane per key)
+    // The table is all zeros (set by cf_create and cf_clear, which synchronize;
+    // cleared by every call that may write the table or hands out its address)
+    bool known_empty;
     uint32_t persistent;    // CF_OPT_PERSISTENT (0 = one tile per CTA, 1 = persistent grid)
     uint32_t chain_hist;    // CF_OPT_CHAIN_HISTOGRAM
 };
@@ -378,10 +381,16 @@ int run_segmented(cf_filter* f, int op, const void* keys, uint64_t n, uint8_t* o
     if (int st = ensure_workspace(f, n, out != nullptr, &w)) return st;
     w.round2_segmented_min = f->round2_min ? f->round2_min : auto_threshold(f, op);
     w.round1_cap = f->round1_cap;
+    // an insert into a table known to be empty: its first chunk's first
+    // round stages zeroed segments instead of loading them
+    bool fresh = op == SEG_INSERT && f->known_empty;
+    f->known_empty = false;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint64_t kb = f->cfg.key_bytes;
     for (uint64_t c0 = 0; c0 < n; c0 += w.cap) {
         const uint64_t m = n - c0 < w.cap ? n - c0 : w.cap;
+        w.fresh = fresh;
+        fresh = false;
         CF_CUDA(f->ops->seg_chunk(dev(f), f->geom, w, op, static_cast<const uint8_t*>(keys) + c0 * kb, m,
                                   out ? out + c0 : nullptr, s, f->cfg.eviction_policy == CF_EVICT_BFS ? 1u : 0u,
                                   f->cfg.max_evictions),
@@ -402,6 +411,7 @@ uint64_t region_threshold(const cf_filter* f, int op) {
 
 int run_region(cf_filter* f, int op, const void* keys, uint64_t n, uint8_t* out, void* stream) {
     if (n == 0) return CF_OK;
+    if (op != SEG_CONTAINS) f->known_empty = false;
     SegWork w{};
     if (int st = ensure_workspace(f, n, op == SEG_CONTAINS || out != nullptr, &w)) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -441,6 +451,7 @@ Path choose_path(const cf_filter* f, int op, uint64_t n, bool sorted_insert) {
 }
 
 int do_insert(cf_filter* f, const void* keys, uint64_t n, uint8_t* out, void* stream) {
+    f->known_empty = false;
     CF_CUDA(f->ops->insert(dev(f), keys, n, out, launch(f, KID_INSERT, stream),
                            f->cfg.eviction_policy == CF_EVICT_BFS ? 1u : 0u, f->cfg.max_evictions),
             "insert launch");
@@ -567,6 +578,7 @@ int cf_create(const cf_config* cfg, uint64_t capacity, cf_filter** out) {
         cf_destroy(f);
         return s;
     }
+    f->known_empty = true;
     *out = f;
     return CF_OK;
 }
@@ -649,6 +661,7 @@ int cf_contains(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, vo
 
 int cf_delete_async(cf_filter* f, const void* d_keys, uint64_t n, uint8_t* d_out, void* stream) {
     if (int s = check_batch(f, d_keys, n)) return s;
+    f->known_empty = false;
     DeviceGuard g(f->device);
     switch (choose_path(f, SEG_DELETE, n, false)) {
         case PATH_REGION: return run_region(f, SEG_DELETE, d_keys, n, d_out, stream);
@@ -674,6 +687,7 @@ int cf_clear(cf_filter* f, void* stream) {
     CF_CUDA(cudaMemsetAsync(f->d_table, 0, f->table_bytes, s), "table clear");
     CF_CUDA(cudaMemsetAsync(f->d_ctr, 0, CTR_COUNT * sizeof(unsigned long long), s), "counter clear");
     CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    f->known_empty = true;
     return CF_OK;
 }
 
@@ -740,6 +754,7 @@ int cf_reset_stats(cf_filter* f) {
 
 int cf_table(cf_filter* f, void** d_table, uint64_t* bytes) {
     if (int s = check_filter(f)) return s;
+    if (d_table) f->known_empty = false;  // the caller may write the table
     if (d_table) *d_table = f->d_table;
     if (bytes) *bytes = f->table_bytes;
     return CF_OK;
@@ -752,6 +767,7 @@ int cf_load_table(cf_filter* f, const void* src, uint64_t bytes, void* stream) {
         return fail(CF_ERR_INVALID, "image is %llu bytes, table is %llu", static_cast<unsigned long long>(bytes),
                     static_cast<unsigned long long>(f->table_bytes));
     DeviceGuard g(f->device);
+    f->known_empty = false;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     CF_CUDA(cudaMemcpyAsync(f->d_table, src, bytes, cudaMemcpyDefault, s), "table load");
     CF_CUDA(cudaMemsetAsync(f->d_ctr + CTR_OCCUPIED, 0, sizeof(unsigned long long), s), "counter reset");
@@ -1001,6 +1017,7 @@ int cf_insert_sorted_noalloc(cf_filter* f, const void* d_keys, uint64_t n, uint8
         return fail(CF_ERR_UNSUPPORTED, "table of %llu segments exceeds the %llu-segment limit of the fixed scratch",
                     static_cast<unsigned long long>(f->geom.nseg), static_cast<unsigned long long>(kNoAllocMaxSegments));
     DeviceGuard g(f->device);
+    f->known_empty = false;
     void* base = nullptr;
     if (int s = noalloc_scratch(&base)) return s;
     SegWork w{};

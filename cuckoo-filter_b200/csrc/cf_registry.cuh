@@ -55,6 +55,9 @@ struct SegWork {
     uint64_t round2_segmented_min;  // list length from which round 2 is segment-staged
     uint32_t round1_cap;            // CF_OPT_ROUND1_CAP (0 = automatic)
     int rg_grid;   // CTAs of the region partition kernels (hist entries: kRgMaxRegions * rg_grid)
+    // Insert into a table known to be all zeros: the first segment round
+    // stages zeroed segments instead of loading them.
+    bool fresh;
 };
 
 // Geometry of the region-staged path: region = bucket >> rl, nreg regions.
@@ -393,7 +396,7 @@ struct Launchers {
     template <int OP>
     static cudaError_t seg_round(const DevTable& t, const SegGeom& g, const SegWork& w, int buf, bool payload,
                                  int round, uint64_t n, bool have_start, bool narrow, cudaStream_t s,
-                                 uint32_t cap = C::bs, int fwd_other = -1, bool ranked = false) {
+                                 uint32_t cap = C::bs, int fwd_other = -1, bool ranked = false, bool fresh = false) {
         if (fwd_other < 0) fwd_other = round == 1 ? 1 : 0;
         // inserts claim slots on a per-bucket mask of at most 64 bits, staged
         // beside the segment; buckets of more slots insert with
@@ -428,7 +431,9 @@ struct Launchers {
         { kern<<<grid, threads, smem, s>>>(t, w.ent[buf], payload ? w.pay[buf] : nullptr, w.start, g.nseg, g.sb_log2,
                                           round, w.ent[other], payload ? w.pay[other] : nullptr,
                                           &w.cnt[round == 3 ? 3 : round - 1], payload ? w.bitmap : nullptr,
-                                          narrow ? 1 : 0, cap, fwd_other, OP == SEG_INSERT ? w.full : nullptr);
+                                          // k_seg: 4-byte entries; k_seg_insert: bit 1, the table is all zeros
+                                          masked ? (fresh ? 2 : 0) : (narrow ? 1 : 0), cap, fwd_other,
+                                          OP == SEG_INSERT ? w.full : nullptr);
           CF_COUNT_LAUNCH(); }
         return cudaGetLastError();
     }
@@ -459,7 +464,9 @@ struct Launchers {
         // batches of at least one key per bucket: slot order within a bucket is unspecified
         const bool ranked = OP == SEG_INSERT && m >= t.nb_mask + 1;
         if (e == cudaSuccess) e = sort_by_segment(true, payload, t, g, w, keys, 0, m, s, &a, &have_start, &narrow);
-        if (e == cudaSuccess) e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, narrow, s, cap1, 1, ranked);
+        if (e == cudaSuccess)
+            e = seg_round<OP>(t, g, w, a, payload, 1, m, have_start, narrow, s, cap1, 1, ranked,
+                              OP == SEG_INSERT && w.fresh);
         // round 2: keys that missed their primary bucket, now in ent/pay[1 - a]
         if (e == cudaSuccess) e = cudaMemcpyAsync(w.h_cnt, w.cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);

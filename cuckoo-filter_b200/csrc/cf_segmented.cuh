@@ -1173,7 +1173,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
                                                             const uint32_t* start, uint64_t nseg, int sb_log2,
                                                             int round, uint64_t* next, uint32_t* next_pay,
                                                             unsigned long long* next_count, uint32_t* bitmap,
-                                                            int /*narrow*/, uint32_t cap, int fwd_other,
+                                                            int flags, uint32_t cap, int fwd_other,
                                                             uint32_t* full) {
     using M = SlotMask<C>;
     static_assert(!RANKED || C::bs <= 16, "ranked claims keep a 16-bit counter above a 16-slot mask");
@@ -1189,6 +1189,7 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
     M* mask = reinterpret_cast<M*>(seg + seg_words);
     uint8_t* seg_bytes = reinterpret_cast<uint8_t*>(seg);
     const uint32_t tid = threadIdx.x, lane = tid & 31;
+    const bool fresh = (flags & 2) != 0;  // the table is all zeros: segments are staged as zeros
     // the segment arrives by one bulk copy completing on this barrier
     __shared__ __align__(8) uint64_t seg_bar;
     if (tid == 0) {
@@ -1209,7 +1210,10 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
         const uint32_t words = nbk * WPB;
         bool staged = true;
         if (tid == 0) bulk_wait_read();  // the previous segment's write-back has read the buffer
-        if (words % 2 == 0) {  // a whole number of 16-byte units: one bulk copy
+        if (fresh) {  // the table is all zeros: no load
+            __syncthreads();
+            for (uint32_t w = tid; w < words; w += blockDim.x) seg[w] = 0;
+        } else if (words % 2 == 0) {  // a whole number of 16-byte units: one bulk copy
             if (tid == 0) {
                 fence_proxy_async_smem();  // earlier accesses of this shared memory come first
                 mbar_arrive_expect_tx(&seg_bar, words * 8u);
@@ -1228,14 +1232,19 @@ __global__ void __launch_bounds__(kSegInsertThreads, 3) k_seg_insert(DevTable t,
             mbar_wait(&seg_bar, seg_phase, kMbarPollLimit);
             break;
         }
-        if (words % 2 == 0) seg_phase ^= 1u;
+        if (!fresh && words % 2 == 0) seg_phase ^= 1u;
         // claim words from the staged segment (ranked: counters at zero)
         auto build_claims = [&]() {
             for (uint32_t b = tid; b < sb; b += blockDim.x)
                 mask[b] = b < nbk ? claimable_slots<C>(empty_mask<C>(seg + static_cast<uint64_t>(b) * WPB), cap)
                                   : static_cast<M>(0);
         };
-        build_claims();
+        if (fresh) {  // every bucket empty: the same claimable slots everywhere
+            const M m0 = claimable_slots<C>(kFull, cap);
+            for (uint32_t b = tid; b < sb; b += blockDim.x) mask[b] = b < nbk ? m0 : static_cast<M>(0);
+        } else {
+            build_claims();
+        }
         __syncthreads();
         // entries per thread per step: 4-byte entries without payloads stay
         // 32-bit in registers, so twice as many fit (half the block barriers)

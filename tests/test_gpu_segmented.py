@@ -318,3 +318,58 @@ def test_round1_cap_option(cfb, orc):
     with pytest.raises(cfb.CuckooError):
         f.setOption(cfb.OPT_ROUND1_CAP, 17)
     f.close()
+
+
+def test_insert_into_known_empty_table_keeps_every_earlier_write(cfb, orc):
+    """The first segment round of an insert into a table the library knows to
+    be all zeros (just created or cleared) stages zeroed segments instead of
+    loading them.  Every call that may write the table drops that knowledge:
+    a second insert, an insert on the random path, a delete, a table load and
+    a chunked batch must all keep what is already stored."""
+    cap = 1 << 22
+    f, o = make(cfb, orc, 8, 16, 16, 0, 500, cap)
+    try:
+        def present(keys):
+            return host_u8(f.containsMany(dev(keys))).all()
+
+        a = orc.splitmix64(301, int(0.4 * cap))
+        b = orc.splitmix64(302, int(0.4 * cap))
+        # fresh table: sorted insert, then a second sorted insert
+        assert f.insertManySorted(dev(a)) == len(a)
+        assert f.insertManySorted(dev(b)) == len(a) + len(b)
+        assert present(a) and present(b) and f.countOccupiedSlots() == len(a) + len(b)
+        # cleared table: only the new keys, counters from zero
+        f.clear()
+        assert f.countOccupiedSlots() == 0
+        assert f.insertManySorted(dev(b)) == len(b) == f.countOccupiedSlots()
+        assert present(b)
+        # a small random-path insert, then a sorted one
+        f.clear()
+        small = orc.splitmix64(303, 1000)
+        f.setOption(cfb.OPT_STAGING, cfb.STAGING_RANDOM)
+        f.insertMany(dev(small))
+        f.setOption(cfb.OPT_STAGING, cfb.STAGING_AUTO)
+        f.insertManySorted(dev(a))
+        assert present(small) and present(a) and f.countOccupiedSlots() == len(small) + len(a)
+        # a delete on a cleared table, then a sorted insert
+        f.clear()
+        f.deleteMany(dev(small))
+        assert f.insertManySorted(dev(a)) == len(a) and present(a)
+        # a loaded table image, then a sorted insert
+        o.insert(b)
+        f.load_table(torch.from_numpy(o.table).cuda())
+        f.insertManySorted(dev(a))
+        assert present(b) and present(a) and f.countOccupiedSlots() == len(a) + len(b)
+    finally:
+        f.close()
+    # a batch in several chunks on a new table: only the first chunk is staged as zeros
+    g, _ = make(cfb, orc, 8, 16, 16, 0, 500, cap)
+    try:
+        g.setOption(cfb.OPT_WORKSPACE_LIMIT, 16 << 20)  # about 1 M keys per chunk
+        both = np.concatenate([a, b])
+        assert g.insertManySorted(dev(both)) == len(both) == g.countOccupiedSlots()
+        assert g.getOption(cfb.OPT_WORKSPACE_BYTES) <= 16 << 20  # the batch ran in chunks
+        assert host_u8(g.containsMany(dev(both))).all()
+        assert g.stats()["failed"] == 0 and g.stats()["lost"] == 0
+    finally:
+        g.close()
