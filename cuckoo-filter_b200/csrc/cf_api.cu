@@ -51,8 +51,10 @@ struct cf_filter {
     uint32_t lookup_kpt;    // CF_OPT_LOOKUP_KPT (0 = default)
     uint32_t probe_width;   // CF_OPT_PROBE_WIDTH (0 or 1 = one lane per key)
     // The table is all zeros (set by cf_create and cf_clear, which synchronize;
-    // cleared by every call that may write the table or hands out its address)
+    // cleared by every call that may write the table).  Never set again once
+    // cf_table has handed out the table's address (table_exposed).
     bool known_empty;
+    bool table_exposed;
     uint32_t persistent;    // CF_OPT_PERSISTENT (0 = one tile per CTA, 1 = persistent grid)
     uint32_t chain_hist;    // CF_OPT_CHAIN_HISTOGRAM
 };
@@ -687,7 +689,7 @@ int cf_clear(cf_filter* f, void* stream) {
     CF_CUDA(cudaMemsetAsync(f->d_table, 0, f->table_bytes, s), "table clear");
     CF_CUDA(cudaMemsetAsync(f->d_ctr, 0, CTR_COUNT * sizeof(unsigned long long), s), "counter clear");
     CF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
-    f->known_empty = true;
+    f->known_empty = !f->table_exposed;
     return CF_OK;
 }
 
@@ -754,7 +756,10 @@ int cf_reset_stats(cf_filter* f) {
 
 int cf_table(cf_filter* f, void** d_table, uint64_t* bytes) {
     if (int s = check_filter(f)) return s;
-    if (d_table) f->known_empty = false;  // the caller may write the table
+    if (d_table) {  // the caller may write the table at any time
+        f->known_empty = false;
+        f->table_exposed = true;
+    }
     if (d_table) *d_table = f->d_table;
     if (bytes) *bytes = f->table_bytes;
     return CF_OK;

@@ -179,7 +179,10 @@ int cf_get_stats(cf_filter* f, cf_stats* out);
 /* Zero all counters except `occupied` (resetEvictionCount(), CuckooFilter.cuh:723). */
 int cf_reset_stats(cf_filter* f);
 
-/* Device pointer to the table image and its size (the reference's d_buckets, :350). */
+/* Device pointer to the table image and its size (the reference's d_buckets, :350).
+ * The caller may write through the pointer at any time: from this call on, the
+ * library no longer assumes that the table is empty after cf_clear (an insert
+ * into a table it knows to be empty skips loading it). */
 int cf_table(cf_filter* f, void** d_table, uint64_t* bytes);
 
 /* Replace the table image with `bytes` bytes from `src` (device or host memory)
