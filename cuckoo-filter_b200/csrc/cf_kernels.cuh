@@ -208,6 +208,35 @@ __device__ __forceinline__ bool plan_insert(const uint64_t (&c)[C::nchunks], uin
     return true;
 }
 
+// The compare-and-swap that tryRemoveAtBucket would try first: clear the
+// first slot holding fp, in the reference's scan order, of bucket image c.
+// False when c does not hold fp.
+template <class C>
+__device__ __forceinline__ bool plan_remove(const uint64_t (&c)[C::nchunks], uint32_t fp, int& w, uint64_t& cur,
+                                            uint64_t& desired) {
+    constexpr uint64_t lane_mask = C::bits == 32 ? 0xFFFFFFFFULL : ((1ULL << C::bits) - 1ULL);
+    if constexpr (!C::chunk_scan) {
+        const SlotMask<C> m = slots_holding<C>(c, fp);
+        if (!m) return false;
+        const uint32_t slot = scan_slot<C>(m, fp);
+        w = static_cast<int>(slot / C::lanes_per_chunk);
+        cur = pick(c, w);
+        desired = cur & ~(lane_mask << ((slot % C::lanes_per_chunk) * C::bits));
+        return true;
+    }
+    const int sw = static_cast<int>((fp & (C::bs - 1)) / C::tpw);
+    const uint64_t rep = replicate<C::bits>(fp);
+    uint32_t words = 0;
+#pragma unroll
+    for (int j = 0; j < C::nchunks; ++j) words |= (zero_lanes<C::bits>(c[j] ^ rep) != 0 ? 1u : 0u) << j;
+    if (!words) return false;
+    w = first_word<C::wc>(words, sw);
+    cur = pick(c, w);
+    const int lane = lowest_lane<C::bits>(zero_lanes<C::bits>(cur ^ rep));
+    desired = cur & ~(lane_mask << (lane * C::bits));
+    return true;
+}
+
 // tryRemoveAtBucket: clear the first slot holding fp.
 template <class C>
 __device__ bool try_remove(uint64_t* bw, uint64_t (&c)[C::nchunks], uint32_t fp, bool& err) {
@@ -525,21 +554,48 @@ __global__ void __launch_bounds__(512) k_delete(DevTable t, const typename C::Ke
             if (k0 + j < n) load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
         }
         uint32_t done = 0;
+        // every key's first compare-and-swap is issued before any result is
+        // checked, so a thread's KPT round trips overlap; a lost race falls
+        // back to tryRemoveAtBucket's retry loop on the refreshed word
+        auto remove_batch = [&](uint32_t live, bool alt) {
+            int w[KPT];
+            uint64_t exp[KPT], des[KPT], old[KPT];
+            uint32_t planned = 0;
+#pragma unroll
+            for (int j = 0; j < KPT; ++j) {
+                w[j] = 0;
+                exp[j] = des[j] = 0;
+                const uint32_t tag = alt ? alt_tag<C>(fp[j]) : fp[j];
+                if (((live >> j) & 1u) && plan_remove<C>(c[j], tag, w[j], exp[j], des[j])) planned |= 1u << j;
+            }
+#pragma unroll
+            for (int j = 0; j < KPT; ++j)
+                if ((planned >> j) & 1u) old[j] = cas64(bucket_words<C>(t, b[j]) + w[j], exp[j], des[j]);
+#pragma unroll
+            for (int j = 0; j < KPT; ++j) {
+                if (!((planned >> j) & 1u)) continue;
+                if (old[j] == exp[j]) {
+                    done |= 1u << j;
+                } else {
+                    put(c[j], w[j], old[j]);
+                    if (try_remove<C>(bucket_words<C>(t, b[j]), c[j], alt ? alt_tag<C>(fp[j]) : fp[j], err))
+                        done |= 1u << j;
+                }
+            }
+        };
+        uint32_t valid = 0;
 #pragma unroll
         for (int j = 0; j < KPT; ++j)
-            if (k0 + j < n && try_remove<C>(bucket_words<C>(t, b[j]), c[j], fp[j], err)) done |= 1u << j;
+            if (k0 + j < n) valid |= 1u << j;
+        remove_batch(valid, false);
 #pragma unroll
         for (int j = 0; j < KPT; ++j) {
-            if (k0 + j < n && !((done >> j) & 1u)) {
+            if (((valid & ~done) >> j) & 1u) {
                 b[j] = alt_bucket<C>(b[j], fp[j], t.nb_mask);
                 load_rlx<C::bucket_bytes>(t.buckets + b[j] * C::bucket_bytes, c[j]);
             }
         }
-#pragma unroll
-        for (int j = 0; j < KPT; ++j)
-            if (k0 + j < n && !((done >> j) & 1u) &&
-                try_remove<C>(bucket_words<C>(t, b[j]), c[j], alt_tag<C>(fp[j]), err))
-                done |= 1u << j;
+        remove_batch(valid & ~done, true);
         removed += __popc(done);
         if (out) store_results<KPT>(out, k0, n, out_vec, done);
     }
