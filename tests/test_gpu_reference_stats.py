@@ -118,9 +118,11 @@ def test_small_config_matches_reference_kernels_statistically(cfb, orc, small_co
 @pytest.mark.parametrize("policy", ["BFS", "DFS"])
 @pytest.mark.parametrize("path,staging", [("plain", "random"), ("sorted", "auto")])
 def test_failures_under_overload_against_reference_kernels(cfb, orc, policy, path, staging):
-    """2^16 slots, maxEvictions 16, 0.995 x capacity keys: thousands of inserts
-    fail in both.  The random path is the reference's own algorithm (two-sided
-    3 sigma); the segment-staged path may only fail less."""
+    """2^16 slots, maxEvictions 16, 0.995 x capacity keys: hundreds to
+    thousands of keys end up absent in both.  The reference drops the tag in
+    hand at every failed DFS walk (CuckooFilter.cuh:953); this library undoes
+    a failed walk, so on either path it may only leave fewer keys absent
+    (failed or lost): one-sided 3 sigma."""
     if orc.ref_gpu() is None:
         pytest.skip("oracle/_ref/libref_gpu.so not built")
     cap = 1 << 16
@@ -136,10 +138,7 @@ def test_failures_under_overload_against_reference_kernels(cfb, orc, policy, pat
     s = 3 * _sigma_diff(mine["absent"], ref["absent"], n) + 3
     msg = f"ours {mine} reference {ref}"
     assert ref["absent"] > 0, msg
-    if staging == "random":
-        assert abs(mine["absent"] - ref["absent"]) <= s, msg
-    else:
-        assert mine["absent"] <= ref["absent"] + s, msg
+    assert mine["absent"] <= ref["absent"] + s, msg
     # a lost tag belonged to some key reported stored: at most that many of
     # them can fail to delete or go missing afterwards
     assert mine["removed"] >= mine["half"] - mine["lost"] and mine["fn_after_delete"] <= mine["lost"], msg
